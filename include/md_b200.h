@@ -1,0 +1,193 @@
+/* md_b200.h — C-ABI of libmdgpu.so, the B200 (sm_100a) implementation of the per-step Lennard-Jones hot path
+ * of nhantran1711/molecular-dynamics: cell list -> Verlet neighbour list -> truncated-shifted LJ forces ->
+ * velocity Verlet with periodic wrap -> rescale / Bussi thermostat -> g(r).
+ *
+ * Plain pointers and sizes only. Every entry point returns an md_status; md_last_error() describes the
+ * last failure on the calling thread. Host pointers passed in are read or written synchronously unless a
+ * function says otherwise. Handles are not thread-safe: calls on one system are serialised on its stream.
+ *
+ * Array layouts (the reference's System layout, include/System.hpp:12-136):
+ *   pos4   n x 4 doubles, particle i at pos4[4 i + k] for k = 0, 1, 2 and a pad at 4 i + 3
+ *   vel3   3 x n doubles, component k of particle i at vel3[k n + i] (likewise force3)
+ *   mass   n doubles;  ids  n uint64 (ids[i] = original index of the particle stored at i)
+ */
+#ifndef MD_B200_H
+#define MD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum md_status {
+    MD_OK = 0,
+    MD_ERR_INVALID = 1,          /* bad argument: null handle or pointer, size mismatch, bad mode */
+    MD_ERR_CUTOFF = 2,           /* 2 r_c > L (src/Forcefield.cpp:18-22) */
+    MD_ERR_LIST_RADIUS = 3,      /* 2 (r_c + skin) > L (src/NeighbourList.cpp:57-59) */
+    MD_ERR_NO_REVERSE_INDEX = 4, /* deterministic forces need a reverse index (src/Forcefield.cpp:217-219) */
+    MD_ERR_CAPACITY = 5,         /* a neighbour row overflowed inside a device-side run; state is undefined */
+    MD_ERR_CUDA = 6,             /* a CUDA runtime call failed */
+    MD_ERR_NO_DEVICE = 7,        /* no usable CUDA device */
+    MD_ERR_STATE = 8,            /* call out of order, e.g. list forces before any list build */
+    MD_ERR_TIMEOUT = 9           /* a bounded device wait gave up */
+} md_status;
+
+/* Precision of the list force kernel */
+typedef enum md_precision {
+    MD_PREC_FP64 = 0,   /* double throughout, bit-identical to the reference's deterministic path */
+    MD_PREC_FP32FX = 1, /* float pair arithmetic, 64-bit fixed-point force accumulation */
+    MD_PREC_FP32 = 2    /* float pair arithmetic, float accumulation */
+} md_precision;
+
+typedef struct md_system md_system;         /* System (include/System.hpp:12) */
+typedef struct md_cells md_cells;           /* CellList (include/CellList.hpp:11) */
+typedef struct md_nlist md_nlist;           /* NeighbourList (include/NeighbourList.hpp:10) */
+typedef struct md_forcefield md_forcefield; /* LennardJonesForceField (include/Forcefield.hpp:6) */
+typedef struct md_rdf md_rdf;               /* RadialDistribution (include/RadialDistribution.hpp:8) */
+
+/* ---- library ------------------------------------------------------------------------------------- */
+const char* md_last_error(void);
+/* Version string and the device the library was built for ("sm_100a"). */
+const char* md_version(void);
+/* Number of CUDA devices visible (0 on a host without a GPU; never fails). */
+int md_device_count(void);
+
+/* ---- System: include/System.hpp:15-125, src/System.cpp ---------------------------------------------- */
+/* System(particles, boxLength) (src/System.cpp:9-29): n particles on `device`, box length L. Ids start at
+ * 0..n-1; velocities, forces and positions start at zero and masses at 1 until uploaded. */
+md_status md_system_create(int64_t n, double box_length, int device, md_system** out);
+md_status md_system_destroy(md_system* s);
+md_status md_system_size(const md_system* s, int64_t* n, double* box_length);
+/* Copy host arrays to the device; any pointer may be NULL to leave that array unchanged. */
+md_status md_system_upload(md_system* s, const double* pos4, const double* vel3, const double* force3,
+                           const double* mass, const uint64_t* ids);
+/* Copy device arrays to the host; any pointer may be NULL. */
+md_status md_system_download(md_system* s, double* pos4, double* vel3, double* force3, double* mass,
+                             uint64_t* ids);
+/* System::reorder (src/System.cpp:42-64): new particle k is old particle order[k]. */
+md_status md_system_reorder(md_system* s, const uint64_t* order);
+/* System::kineticEnergy (src/System.cpp:67-76), same 1024-block summation order (include/Parallel.hpp:32-57). */
+md_status md_kinetic_energy(md_system* s, double* out);
+/* System::temperature (src/System.cpp:79-82). */
+md_status md_temperature(md_system* s, double* out);
+/* System::stateHash (src/System.cpp:85-105): FNV-1a of every position and velocity bit pattern. */
+md_status md_state_hash(md_system* s, uint64_t* out);
+/* Multiply every velocity component by `scale` (src/Thermostat.cpp:6-12). */
+md_status md_scale_velocities(md_system* s, double scale);
+/* rescaleVelocities (src/Thermostat.cpp:17-30), computed on the device from the device kinetic energy. */
+md_status md_rescale_velocities(md_system* s, double target_temperature);
+/* BussiThermostat::apply(system, dt) (src/Thermostat.cpp:36-58) for a thermostat of coupling time tau, with
+ * the draws r1 ~ N(0,1) and chi2 ~ Gamma(0.5 (dof-1), 2) supplied by the caller (md_bussi_noise makes them
+ * from the reference's seed). */
+md_status md_bussi_apply(md_system* s, double temperature, double tau, double dt, double r1, double chi2);
+/* The (r1, chi2) draws of `count` successive BussiThermostat::apply calls on a system of n particles from
+ * std::mt19937_64(seed) (src/Thermostat.cpp:48-51): r1[k], chi2[k]. Host-only, no device needed. */
+md_status md_bussi_noise(uint64_t seed, int64_t n, int64_t count, double* r1, double* chi2);
+
+/* ---- Initialisation: include/Initialisation.hpp:9-12, src/Initialisation.cpp (host input set-up) ----- */
+/* createFCCLattice (src/Initialisation.cpp:7-44): 4 cells^3 particles offset by a/4, into pos4 (host). */
+md_status md_fcc_lattice(int cells, double lattice_constant, double* pos4);
+/* initializeVelocities (src/Initialisation.cpp:47-76): Maxwell-Boltzmann draws from std::mt19937(seed) on the
+ * host, centre-of-mass removal, then rescaleVelocities on the device. Uses the system's masses. */
+md_status md_initialize_velocities(md_system* s, double temperature, uint32_t seed);
+
+/* ---- streams, timing and counters ---------------------------------------------------------------------- */
+/* The cudaStream_t every call on this system is queued on (for CUDA events around calls). */
+md_status md_system_stream(md_system* s, void** stream);
+/* Wait for all work queued on the system's stream. */
+md_status md_system_synchronize(md_system* s);
+/* Kernels this system has launched so far (every kernel of this library counts one). */
+md_status md_system_launch_count(const md_system* s, uint64_t* launches);
+/* While enabled, md_run brackets each list force kernel with CUDA events on the system's stream;
+ * md_profile_read returns their summed time (ms) and count since the last enable. */
+md_status md_profile_enable(md_system* s, int enable);
+md_status md_profile_read(md_system* s, double* force_ms, int64_t* force_launches);
+
+/* ---- CellList: include/CellList.hpp:14-40, src/CellList.cpp ----------------------------------------- */
+md_status md_cells_create(double min_cell_size, md_cells** out);
+md_status md_cells_destroy(md_cells* c);
+/* CellList::build (src/CellList.cpp:9-52) on the system's current positions (the system is not reordered). */
+md_status md_cells_build(md_cells* c, md_system* s, int* cells_per_side);
+/* particle_cell[n] = cellOf(i); cell_start[ncells + 1]; cell_particles[n] = sortedOrder(). Any may be NULL. */
+md_status md_cells_download(md_cells* c, int* particle_cell, uint64_t* cell_start, uint64_t* cell_particles);
+
+/* ---- NeighbourList: include/NeighbourList.hpp:15-49, src/NeighbourList.cpp -------------------------- */
+/* NeighbourList(cutOff, skin, reverseIndex) (src/NeighbourList.cpp:5-8). */
+md_status md_nlist_create(double cutoff, double skin, int reverse_index, md_nlist** out);
+md_status md_nlist_destroy(md_nlist* nl);
+/* NeighbourList::build (src/NeighbourList.cpp:55-134): sorts the system by cell (reorders it) and rebuilds. */
+md_status md_nlist_build(md_nlist* nl, md_system* s);
+/* NeighbourList::update (src/NeighbourList.cpp:11-36): rebuild if any particle moved more than skin/2. */
+md_status md_nlist_update(md_nlist* nl, md_system* s, int* rebuilt);
+/* getPairCount, getRebuildCount, the cell grid side of the last build, hasReverseIndex. Any may be NULL. */
+md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_count, int* cells_per_side,
+                        int* reverse_index);
+/* The half list in the reference's CSR form: offsets[n + 1] (firstPairOf), neighbours[pairs]
+ * (neighboursOf in candidate order) and, when the list has a reverse index, rev_offsets[n + 1] and
+ * rev_pairs[pairs] (pairsAsSecond). Any may be NULL. */
+md_status md_nlist_download(md_nlist* nl, uint64_t* offsets, uint64_t* neighbours, uint64_t* rev_offsets,
+                            uint64_t* rev_pairs);
+
+/* ---- LennardJonesForceField: include/Forcefield.hpp:8-45, src/Forcefield.cpp ------------------------ */
+/* LennardJonesForceField(epsilon, sigma, cut_off) (src/Forcefield.cpp:8-15). Precision starts at MD_PREC_FP64. */
+md_status md_forcefield_create(double epsilon, double sigma, double cutoff, md_forcefield** out);
+md_status md_forcefield_destroy(md_forcefield* ff);
+/* getEnergyShift (include/Forcefield.hpp:21-24). */
+md_status md_forcefield_shift(const md_forcefield* ff, double* shift);
+/* Precision of the list path; setMixedPrecision(true) (include/Forcefield.hpp:39-41) maps to MD_PREC_FP32FX. */
+md_status md_forcefield_set_precision(md_forcefield* ff, int precision);
+/* setDeterministic (include/Forcefield.hpp:43-45): with it, list forces require a list built with
+ * reverseIndex, as in the reference. Every precision is deterministic on the device regardless. */
+md_status md_forcefield_set_deterministic(md_forcefield* ff, int deterministic);
+/* computeForces(System&, const NeighbourList&) (src/Forcefield.cpp:81-326): writes the system's forces and
+ * returns PE, the virial W (getVirial) and the inside-cutoff pair count (getInsidePairs). Outputs may be NULL. */
+md_status md_forces_list(md_forcefield* ff, md_system* s, md_nlist* nl, double* pe, double* virial,
+                         double* inside);
+/* computeForces(System&), the O(N^2) path (src/Forcefield.cpp:39-78). */
+md_status md_forces_all_pairs(md_forcefield* ff, md_system* s, double* pe, double* virial, double* inside);
+
+/* ---- VelocityVerletIntegrator: include/Integrator.hpp:9-19, src/Integrator.cpp --------------------- */
+/* step(System&, const LennardJonesForceField&, NeighbourList&) (src/Integrator.cpp:18-30): half kick, drift
+ * and wrap, list update, forces, half kick. Returns the new PE; `rebuilt` says whether the list was rebuilt. */
+md_status md_step_list(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, double* pe, int* rebuilt);
+/* step(System&, const LennardJonesForceField&) with O(N^2) forces (src/Integrator.cpp:7-16). */
+md_status md_step_all_pairs(md_system* s, md_forcefield* ff, double dt, double* pe);
+
+/* Device-resident run of n_steps list steps with no host round trip per step (md_sim's loops,
+ * src/main.cpp:219-304). Per step, in order: step_list; then the optional thermostat; then the optional
+ * g(r) sample. Outputs (each NULL or n_steps long, host memory): pe[k] the step's PE, ke[k] the kinetic
+ * energy after the thermostat, virial[k]. */
+typedef struct md_run_options {
+    int thermostat;             /* 0 none (NVE), 1 rescale, 2 Bussi */
+    int rescale_every;          /* rescale when (first_step + k) % rescale_every == 0 */
+    double rescale_temperature; /* target of the rescale */
+    int melt_until;             /* rescale to melt_temperature instead while first_step + k <= melt_until */
+    double melt_temperature;
+    double bussi_temperature;   /* Bussi target temperature */
+    double bussi_tau;           /* coupling time; c = exp(-dt / tau) as in src/Thermostat.cpp:46 */
+    const double* bussi_r1;     /* n_steps draws (host), e.g. from md_bussi_noise */
+    const double* bussi_chi2;
+    md_rdf* rdf;                /* sample g(r) when (first_step + k) % rdf_every == 0 (NULL: never) */
+    int rdf_every;
+    int64_t first_step;         /* step number of the first step of this run (1-based, as md_sim counts) */
+} md_run_options;
+md_status md_run(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
+                 const md_run_options* opts, double* pe, double* ke, double* virial);
+
+/* ---- RadialDistribution: include/RadialDistribution.hpp:10-20, src/RadialDistribution.cpp ----------- */
+md_status md_rdf_create(double r_max, int bins, md_rdf** out);
+md_status md_rdf_destroy(md_rdf* r);
+/* RadialDistribution::sample (src/RadialDistribution.cpp:11-30) over the list's half pairs. */
+md_status md_rdf_sample(md_rdf* r, md_system* s, md_nlist* nl);
+/* radii (src/RadialDistribution.cpp:32-38) and values (:42-54); either may be NULL; bins long. */
+md_status md_rdf_values(md_rdf* r, double* radii, double* g, int* samples);
+/* The raw histogram of pair counts (bins long). */
+md_status md_rdf_histogram(md_rdf* r, double* hist);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MD_B200_H */

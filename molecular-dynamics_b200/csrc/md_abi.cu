@@ -1,0 +1,1110 @@
+// libmdgpu: the C-ABI (include/md_b200.h) over the sm_100a kernels. Host orchestration only: handles own
+// their device buffers and one CUDA stream per system; every kernel is in the md_*.cuh headers.
+#include "md_b200.h"
+
+#include "md_cells.cuh"
+#include "md_common.cuh"
+#include "md_fp32.cuh"
+#include "md_fp64.cuh"
+#include "md_nlist.cuh"
+#include "md_scan.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+using namespace md;
+
+namespace {
+
+thread_local std::string g_error;
+thread_local uint64_t* g_launches = nullptr;  // launch counter of the system the current call works on
+
+md_status fail(md_status s, const std::string& msg) {
+    g_error = msg;
+    return s;
+}
+
+#define MD_CUDA(call)                                                                                  \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) return fail(MD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// After k kernel launches: surface launch errors and count the launches
+#define MD_CHECK_LAUNCH_N(k)                    \
+    do {                                        \
+        MD_CUDA(cudaGetLastError());            \
+        if (g_launches) *g_launches += (k);     \
+    } while (0)
+#define MD_CHECK_LAUNCH() MD_CHECK_LAUNCH_N(1)
+// exclusive_scan launches three kernels
+#define MD_CHECK_SCAN() MD_CHECK_LAUNCH_N(3)
+
+#define MD_TRY(expr)                       \
+    do {                                   \
+        md_status s_ = (expr);             \
+        if (s_ != MD_OK) return s_;        \
+    } while (0)
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t count = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        count = 0;
+    }
+    // Grow to at least n elements (contents are not kept)
+    cudaError_t reserve(size_t n) {
+        if (n <= count && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
+        if (e == cudaSuccess) count = std::max<size_t>(n, 1);
+        return e;
+    }
+};
+
+inline unsigned blocks_for(long long n, int threads) {
+    return static_cast<unsigned>((n + threads - 1) / threads);
+}
+
+constexpr int kThreads = 256;
+
+// Slots of md_system::scal (device scalars)
+constexpr int kScalFactor = 1;  // [1] velocity scale factor, [2] 1 to apply it / 0 to skip
+constexpr int kScalKE = 4;      // [4] kinetic energy ([5] scratch of the blocked sum)
+constexpr int kScalR1 = 6;      // [6] r1, [7] chi2 of one Bussi step
+
+}  // namespace
+
+// ---- handles ---------------------------------------------------------------------------------------------
+
+struct md_system {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int64_t n = 0;
+    Box box{};
+    DevBuf<double4> pos, pos2;
+    DevBuf<double> vel, vel2, force, force2, mass, mass2;
+    DevBuf<uint64_t> ids, ids2;
+    DevBuf<double2> ke_blocks;
+    DevBuf<double> scal;         // device scalars, indexed by the kScal* constants
+    double* host_scal = nullptr; // pinned mirror of scal
+    uint64_t layout = 0;         // bumps whenever the particle order changes
+    uint64_t launches = 0;       // kernels launched on this system
+    // md_profile_*: events around each list force kernel of md_run
+    bool profile = false;
+    std::vector<cudaEvent_t> events;
+    size_t events_used = 0;
+    double profile_ms = 0.0;
+    int64_t profile_count = 0;
+};
+
+struct CellGrid {
+    int ncps = 0, ncells = 0;
+    DevBuf<int> cell_of, count, start, cursor;
+    DevBuf<uint32_t> bucket, order;
+    DevBuf<long long> tiles;
+};
+
+struct md_cells {
+    double min_size = 0.0;
+    int device = -1;
+    int64_t n = 0;
+    CellGrid g;
+};
+
+struct md_nlist {
+    double rc = 0, skin = 0, rl = 0, rl2 = 0, max_disp2 = 0;
+    bool reverse = false;
+    int device = -1;
+    const md_system* sys = nullptr;
+    uint64_t layout = 0;  // sys->layout right after our last build
+    int64_t n = -1;
+    CellGrid grid;
+    int cap = 0;
+    bool use_cells = false;
+    DevBuf<uint32_t> rows;
+    DevBuf<int2> counts;
+    DevBuf<int> tmp_counts, cell_sorted, flags;  // flags: [0] stale, [1] max row, [2] device rebuild count
+    DevBuf<long long> half_off, rev_off, tiles;
+    DevBuf<double4> ref_pos;
+    DevBuf<float4> frames;  // per-particle float coordinates for the float kernels (n + 1, sentinel last)
+    int rebuilds = 0;
+    uint64_t pairs = 0;
+    bool built = false;
+};
+
+struct md_forcefield {
+    double eps = 1, sigma = 1, rc = 2.5;
+    LJ lj{};
+    int precision = MD_PREC_FP64;
+    bool deterministic = false;
+    double virial = 0.0, inside = 0.0;
+    int device = -1;
+    DevBuf<double2> eblocks;
+    DevBuf<double> out;  // [0] pe, [1] virial, [2] inside
+    DevBuf<unsigned long long> inside_count;
+    DevBuf<long long> fx_acc;  // fixed-point accumulators of the float kernels: pe, virial
+    double* host_out = nullptr;
+};
+
+struct md_rdf {
+    double rmax = 0, bin_width = 0;
+    int bins = 0;
+    int samples = 0;
+    double particles = 0, density = 0;
+    int device = -1;
+    DevBuf<unsigned long long> hist;
+};
+
+namespace {
+
+md_status use_device(int device) {
+    MD_CUDA(cudaSetDevice(device));
+    return MD_OK;
+}
+
+// Select the system's device and count the call's launches on it
+md_status use_system(md_system* s) {
+    g_launches = &s->launches;
+    MD_CUDA(cudaSetDevice(s->device));
+    return MD_OK;
+}
+
+md_status sync(md_system* s) {
+    MD_CUDA(cudaStreamSynchronize(s->stream));
+    MD_CUDA(cudaGetLastError());
+    return MD_OK;
+}
+
+// Kinetic energy into s->scal[0] with the reference's blocked order (no host sync)
+md_status kinetic_async(md_system* s) {
+    const int n = static_cast<int>(s->n);
+    const int nb = (n + kChunk - 1) / kChunk;
+    if (nb == 0) {
+        MD_CUDA(cudaMemsetAsync(s->scal.p + kScalKE, 0, sizeof(double), s->stream));
+        return MD_OK;
+    }
+    MD_CUDA(s->ke_blocks.reserve(nb));
+    const size_t smem = kEnergyWarps * kChunk * sizeof(double);
+    k_kinetic_blocks<<<blocks_for(nb, kEnergyWarps), kEnergyWarps * 32, smem, s->stream>>>(s->vel.p, s->mass.p, n,
+                                                                                          s->ke_blocks.p, nb);
+    MD_CHECK_LAUNCH();
+    k_sum_blocks<<<1, 32, 0, s->stream>>>(s->ke_blocks.p, nb, s->scal.p + kScalKE);
+    MD_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+md_status scale_async(md_system* s) {
+    const long long count = 3 * s->n;
+    if (count == 0) return MD_OK;
+    const unsigned g = std::min<unsigned>(blocks_for(count, kThreads), 148u * 16u);
+    k_scale_velocities<<<g, kThreads, 0, s->stream>>>(s->vel.p, count, s->scal.p + kScalFactor);
+    MD_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+double dof_of(int64_t n) { return 3.0 * static_cast<double>(n) - 3.0; }
+
+// Counting sort by cell (src/CellList.cpp:9-52) into g.start / g.order; returns ncps
+md_status cell_sort(CellGrid& g, md_system* s, double min_size) {
+    const int n = static_cast<int>(s->n);
+    const double L = s->box.L;
+    g.ncps = std::max(1, static_cast<int>(L / min_size));  // src/CellList.cpp:14
+    const long long nc = static_cast<long long>(g.ncps) * g.ncps * g.ncps;
+    if (nc > (1ll << 30)) return fail(MD_ERR_INVALID, "cell grid too large");
+    g.ncells = static_cast<int>(nc);
+    const double inv_cell = g.ncps / L;  // src/CellList.cpp:18
+    MD_CUDA(g.cell_of.reserve(n));
+    MD_CUDA(g.count.reserve(g.ncells));
+    MD_CUDA(g.cursor.reserve(g.ncells));
+    MD_CUDA(g.start.reserve(g.ncells + 1));
+    MD_CUDA(g.bucket.reserve(n));
+    MD_CUDA(g.order.reserve(n));
+    MD_CUDA(g.tiles.reserve(scan_tiles_needed(g.ncells)));
+    MD_CUDA(cudaMemsetAsync(g.count.p, 0, sizeof(int) * g.ncells, s->stream));
+    MD_CUDA(cudaMemsetAsync(g.cursor.p, 0, sizeof(int) * g.ncells, s->stream));
+    if (n > 0) {
+        k_cell_assign<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(s->pos.p, n, inv_cell, g.ncps, g.cell_of.p,
+                                                                           g.count.p);
+        MD_CHECK_LAUNCH();
+    }
+    exclusive_scan<int, int>(g.count.p, g.ncells, g.start.p, g.tiles.p, s->stream);
+    MD_CHECK_SCAN();
+    if (n > 0) {
+        k_cell_scatter<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(g.cell_of.p, n, g.start.p, g.cursor.p,
+                                                                            g.bucket.p);
+        MD_CHECK_LAUNCH();
+        k_cell_rank<<<blocks_for(static_cast<long long>(g.ncells) * 32, kThreads), kThreads, 0, s->stream>>>(
+            g.start.p, g.ncells, g.bucket.p, g.order.p);
+        MD_CHECK_LAUNCH();
+    }
+    return MD_OK;
+}
+
+int initial_capacity(const md_nlist* nl, const md_system* s) {
+    const double vol = s->box.L * s->box.L * s->box.L;
+    const double rho = static_cast<double>(s->n) / vol;
+    double est = 4.18879020478639 * nl->rl2 * nl->rl * rho;  // full sphere of radius r_l
+    est = std::min(est, static_cast<double>(s->n));
+    int cap = static_cast<int>(1.35 * est) + 24;
+    return (cap + 7) & ~7;
+}
+
+// NeighbourList::build (src/NeighbourList.cpp:55-134) on the device. The reference builds the cell list,
+// reorders the system, and builds the cell list again; the second build only recomputes the cells of the
+// already sorted particles (same positions, identity order), which k_permute_commit writes directly.
+md_status nlist_build(md_nlist* nl, md_system* s) {
+    if (2.0 * nl->rl > s->box.L) return fail(MD_ERR_LIST_RADIUS, "Cutoff + skin must be less than half the box length");
+    const int n = static_cast<int>(s->n);
+    nl->device = s->device;
+    MD_TRY(cell_sort(nl->grid, s, nl->rl));
+    MD_CUDA(s->pos2.reserve(n));
+    MD_CUDA(s->vel2.reserve(3 * static_cast<size_t>(n)));
+    MD_CUDA(s->force2.reserve(3 * static_cast<size_t>(n)));
+    MD_CUDA(s->mass2.reserve(n));
+    MD_CUDA(s->ids2.reserve(n));
+    MD_CUDA(nl->cell_sorted.reserve(n));
+    MD_CUDA(nl->ref_pos.reserve(n));
+    if (n > 0) {
+        k_permute<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(
+            nl->grid.order.p, n, s->pos.p, s->vel.p, s->force.p, s->mass.p, s->ids.p, s->pos2.p, s->vel2.p,
+            s->force2.p, s->mass2.p, s->ids2.p);
+        MD_CHECK_LAUNCH();
+        k_permute_commit<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(
+            n, nl->grid.order.p, nl->grid.cell_of.p, s->pos2.p, s->vel2.p, s->force2.p, s->mass2.p, s->ids2.p,
+            s->pos.p, s->vel.p, s->force.p, s->mass.p, s->ids.p, nl->cell_sorted.p, nl->ref_pos.p);
+        MD_CHECK_LAUNCH();
+    }
+    s->layout++;
+    nl->use_cells = nl->grid.ncps >= 3;  // src/NeighbourList.cpp:69
+    if (nl->cap == 0 || nl->n != s->n) nl->cap = initial_capacity(nl, s);
+    MD_CUDA(nl->counts.reserve(n));
+    MD_CUDA(nl->flags.reserve(4));
+    MD_CUDA(nl->half_off.reserve(n + 1));
+    MD_CUDA(nl->tmp_counts.reserve(n));
+    MD_CUDA(nl->tiles.reserve(scan_tiles_needed(n)));
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        MD_CUDA(nl->rows.reserve(static_cast<size_t>(n) * nl->cap));
+        MD_CUDA(cudaMemsetAsync(nl->flags.p, 0, 4 * sizeof(int), s->stream));
+        ListGeom geo{s->box, nl->rl2, nl->grid.ncps, nl->use_cells ? 1 : 0, nl->cap, static_cast<uint32_t>(n)};
+        if (n > 0) {
+            k_nlist_build<<<blocks_for(n, 128), 128, 0, s->stream>>>(s->pos.p, n, geo, nl->cell_sorted.p,
+                                                                      nl->grid.start.p, nl->rows.p, nl->counts.p,
+                                                                      nl->flags.p + 1);
+            MD_CHECK_LAUNCH();
+        }
+        int maxrow = 0;
+        MD_CUDA(cudaMemcpyAsync(&maxrow, nl->flags.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        MD_TRY(sync(s));
+        if (maxrow <= nl->cap) break;
+        nl->cap = ((maxrow + maxrow / 4 + 16) + 7) & ~7;
+        if (attempt == 3) return fail(MD_ERR_CAPACITY, "neighbour row capacity could not be met");
+    }
+    if (n > 0) {
+        k_own_counts<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(nl->counts.p, n, nl->tmp_counts.p);
+        MD_CHECK_LAUNCH();
+    }
+    exclusive_scan<int, long long>(nl->tmp_counts.p, n, nl->half_off.p, nl->tiles.p, s->stream);
+    MD_CHECK_SCAN();
+    long long pairs = 0;
+    MD_CUDA(cudaMemcpyAsync(&pairs, nl->half_off.p + n, sizeof(long long), cudaMemcpyDeviceToHost, s->stream));
+    MD_TRY(sync(s));
+    nl->pairs = static_cast<uint64_t>(pairs);
+    nl->n = s->n;
+    nl->sys = s;
+    nl->layout = s->layout;
+    nl->built = true;
+    nl->rebuilds++;
+    return MD_OK;
+}
+
+bool nlist_current(const md_nlist* nl, const md_system* s) {
+    return nl->built && nl->sys == s && nl->n == s->n && nl->layout == s->layout;
+}
+
+// Defined in md_abi_float.inl and below
+md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy);
+md_status rdf_sample_async(md_rdf* r, md_system* s, md_nlist* nl);
+md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
+                    const md_run_options& o, double* pe, double* ke, double* virial);
+
+md_status check_cutoff(const md_forcefield* ff, const md_system* s) {
+    if (2.0 * ff->rc > s->box.L) return fail(MD_ERR_CUTOFF, "Cutoff must be less than half the box length");
+    return MD_OK;
+}
+
+// md_profile_*: a CUDA event on the system's stream before and after each list force kernel
+md_status profile_mark(md_system* s) {
+    if (!s->profile) return MD_OK;
+    if (s->events_used == s->events.size()) {
+        cudaEvent_t e;
+        MD_CUDA(cudaEventCreate(&e));
+        s->events.push_back(e);
+    }
+    MD_CUDA(cudaEventRecord(s->events[s->events_used++], s->stream));
+    return MD_OK;
+}
+
+// Sum the (start, end) event pairs recorded so far; the stream must have been synchronised
+md_status profile_collect(md_system* s) {
+    for (size_t k = 0; k + 1 < s->events_used; k += 2) {
+        float ms = 0.f;
+        MD_CUDA(cudaEventElapsedTime(&ms, s->events[k], s->events[k + 1]));
+        s->profile_ms += ms;
+        s->profile_count++;
+    }
+    s->events_used = 0;
+    return MD_OK;
+}
+
+// List forces into s->force; energies (pe, virial, inside) into ff->out on the device when want_energy
+md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy) {
+    const int n = static_cast<int>(s->n);
+    MD_CUDA(ff->out.reserve(4));
+    MD_CUDA(ff->inside_count.reserve(1));
+    MD_CUDA(cudaMemsetAsync(ff->inside_count.p, 0, sizeof(unsigned long long), s->stream));
+    if (ff->precision == MD_PREC_FP64) {
+        if (n > 0) {
+            MD_TRY(profile_mark(s));
+            k_force_fp64<<<blocks_for(n, 128), 128, 0, s->stream>>>(s->pos.p, n, s->box, ff->lj, nl->rows.p, nl->cap,
+                                                                     nl->counts.p, s->force.p, ff->inside_count.p);
+            MD_CHECK_LAUNCH();
+            MD_TRY(profile_mark(s));
+        }
+        if (want_energy) {
+            const long long pairs = static_cast<long long>(nl->pairs);
+            const int nb = static_cast<int>((pairs + kChunk - 1) / kChunk);
+            if (nb > 0) {
+                MD_CUDA(ff->eblocks.reserve(nb));
+                const size_t smem = kEnergyWarps * kChunk * sizeof(double2);
+                MD_CUDA(cudaFuncSetAttribute(k_energy_blocks_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem)));
+                k_energy_blocks_fp64<<<blocks_for(nb, kEnergyWarps), kEnergyWarps * 32, smem, s->stream>>>(
+                    s->pos.p, n, s->box, ff->lj, nl->rows.p, nl->cap, nl->half_off.p, pairs, ff->eblocks.p, nb);
+                MD_CHECK_LAUNCH();
+                k_sum_blocks<<<1, 32, 0, s->stream>>>(ff->eblocks.p, nb, ff->out.p);
+                MD_CHECK_LAUNCH();
+            } else {
+                MD_CUDA(cudaMemsetAsync(ff->out.p, 0, 2 * sizeof(double), s->stream));
+            }
+        }
+    } else {
+        MD_TRY(forces_list_float_async(ff, s, nl, want_energy));
+    }
+    return MD_OK;
+}
+
+md_status read_energy(md_forcefield* ff, md_system* s, double* pe, double* virial, double* inside) {
+    unsigned long long ins = 0;
+    double out[2] = {0, 0};
+    MD_CUDA(cudaMemcpyAsync(out, ff->out.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    MD_CUDA(cudaMemcpyAsync(&ins, ff->inside_count.p, sizeof(ins), cudaMemcpyDeviceToHost, s->stream));
+    MD_TRY(sync(s));
+    ff->virial = out[1];
+    ff->inside = static_cast<double>(ins);
+    if (pe) *pe = out[0];
+    if (virial) *virial = out[1];
+    if (inside) *inside = ff->inside;
+    return MD_OK;
+}
+
+md_status kick_drift_async(md_system* s, md_nlist* nl, double dt, bool check_skin) {
+    const int n = static_cast<int>(s->n);
+    if (n == 0) return MD_OK;
+    if (check_skin) MD_CUDA(cudaMemsetAsync(nl->flags.p, 0, sizeof(int), s->stream));
+    k_kick_drift<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(
+        s->pos.p, s->vel.p, s->force.p, s->mass.p, n, 0.5 * dt, dt, s->box, check_skin ? nl->ref_pos.p : nullptr,
+        nl ? nl->max_disp2 : 0.0, check_skin ? nl->flags.p : nullptr);
+    MD_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+md_status kick_async(md_system* s, double dt) {
+    const int n = static_cast<int>(s->n);
+    if (n == 0) return MD_OK;
+    k_kick<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(s->vel.p, s->force.p, s->mass.p, n, 0.5 * dt);
+    MD_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+}  // namespace
+
+#include "md_abi_float.inl"
+
+// ---- library ---------------------------------------------------------------------------------------------
+
+extern "C" {
+
+const char* md_last_error(void) { return g_error.c_str(); }
+
+const char* md_version(void) { return "md-b200 0.1 (sm_100a)"; }
+
+int md_device_count(void) {
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return c;
+}
+
+// ---- System ------------------------------------------------------------------------------------------------
+
+md_status md_system_create(int64_t n, double box_length, int device, md_system** out) {
+    if (!out || n < 0 || n > kMaxParticles || !(box_length > 0.0)) return fail(MD_ERR_INVALID, "md_system_create: bad arguments");
+    if (md_device_count() <= device || device < 0) return fail(MD_ERR_NO_DEVICE, "no CUDA device " + std::to_string(device));
+    MD_TRY(use_device(device));
+    auto* s = new md_system;
+    s->device = device;
+    s->n = n;
+    s->box = Box{box_length, 1.0 / box_length, 0.25 * box_length};
+    md_status st = MD_OK;
+    auto chk = [&](cudaError_t e) {
+        if (e != cudaSuccess && st == MD_OK) st = fail(MD_ERR_CUDA, cudaGetErrorString(e));
+    };
+    chk(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    chk(s->pos.reserve(n));
+    chk(s->vel.reserve(3 * n));
+    chk(s->force.reserve(3 * n));
+    chk(s->mass.reserve(n));
+    chk(s->ids.reserve(n));
+    chk(s->scal.reserve(8));
+    chk(cudaMallocHost(reinterpret_cast<void**>(&s->host_scal), 8 * sizeof(double)));
+    if (st == MD_OK && n > 0) {
+        chk(cudaMemsetAsync(s->pos.p, 0, sizeof(double4) * n, s->stream));
+        chk(cudaMemsetAsync(s->vel.p, 0, sizeof(double) * 3 * n, s->stream));
+        chk(cudaMemsetAsync(s->force.p, 0, sizeof(double) * 3 * n, s->stream));
+        std::vector<double> ones(n, 1.0);
+        std::vector<uint64_t> ids(n);
+        for (int64_t i = 0; i < n; ++i) ids[i] = static_cast<uint64_t>(i);
+        chk(cudaMemcpyAsync(s->mass.p, ones.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+        chk(cudaMemcpyAsync(s->ids.p, ids.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s->stream));
+        chk(cudaStreamSynchronize(s->stream));
+    }
+    if (st != MD_OK) {
+        md_system_destroy(s);
+        return st;
+    }
+    *out = s;
+    return MD_OK;
+}
+
+md_status md_system_destroy(md_system* s) {
+    if (!s) return MD_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (cudaEvent_t e : s->events) cudaEventDestroy(e);
+    if (s->host_scal) cudaFreeHost(s->host_scal);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return MD_OK;
+}
+
+md_status md_system_size(const md_system* s, int64_t* n, double* box_length) {
+    if (!s) return fail(MD_ERR_INVALID, "null system");
+    if (n) *n = s->n;
+    if (box_length) *box_length = s->box.L;
+    return MD_OK;
+}
+
+md_status md_system_upload(md_system* s, const double* pos4, const double* vel3, const double* force3,
+                           const double* mass, const uint64_t* ids) {
+    if (!s) return fail(MD_ERR_INVALID, "null system");
+    MD_TRY(use_system(s));
+    const size_t n = static_cast<size_t>(s->n);
+    if (n == 0) return MD_OK;
+    if (pos4) MD_CUDA(cudaMemcpyAsync(s->pos.p, pos4, sizeof(double4) * n, cudaMemcpyHostToDevice, s->stream));
+    if (vel3) MD_CUDA(cudaMemcpyAsync(s->vel.p, vel3, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s->stream));
+    if (force3) MD_CUDA(cudaMemcpyAsync(s->force.p, force3, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s->stream));
+    if (mass) MD_CUDA(cudaMemcpyAsync(s->mass.p, mass, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+    if (ids) MD_CUDA(cudaMemcpyAsync(s->ids.p, ids, sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s->stream));
+    // New positions keep the particle order, so a list built before stays usable until update() says it is
+    // stale, as with System::setPosition in the reference
+    return sync(s);
+}
+
+md_status md_system_download(md_system* s, double* pos4, double* vel3, double* force3, double* mass, uint64_t* ids) {
+    if (!s) return fail(MD_ERR_INVALID, "null system");
+    MD_TRY(use_system(s));
+    const size_t n = static_cast<size_t>(s->n);
+    if (n == 0) return MD_OK;
+    if (pos4) MD_CUDA(cudaMemcpyAsync(pos4, s->pos.p, sizeof(double4) * n, cudaMemcpyDeviceToHost, s->stream));
+    if (vel3) MD_CUDA(cudaMemcpyAsync(vel3, s->vel.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s->stream));
+    if (force3) MD_CUDA(cudaMemcpyAsync(force3, s->force.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s->stream));
+    if (mass) MD_CUDA(cudaMemcpyAsync(mass, s->mass.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+    if (ids) MD_CUDA(cudaMemcpyAsync(ids, s->ids.p, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost, s->stream));
+    return sync(s);
+}
+
+md_status md_system_reorder(md_system* s, const uint64_t* order) {
+    if (!s || (!order && s->n)) return fail(MD_ERR_INVALID, "md_system_reorder: bad arguments");
+    MD_TRY(use_system(s));
+    const int n = static_cast<int>(s->n);
+    if (n == 0) return MD_OK;
+    std::vector<uint32_t> o(n);
+    std::vector<char> seen(n, 0);
+    for (int k = 0; k < n; ++k) {
+        if (order[k] >= static_cast<uint64_t>(n) || seen[order[k]]) return fail(MD_ERR_INVALID, "order is not a permutation");
+        seen[order[k]] = 1;
+        o[k] = static_cast<uint32_t>(order[k]);
+    }
+    DevBuf<uint32_t> d;
+    MD_CUDA(d.reserve(n));
+    MD_CUDA(cudaMemcpyAsync(d.p, o.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s->stream));
+    MD_CUDA(s->pos2.reserve(n));
+    MD_CUDA(s->vel2.reserve(3 * static_cast<size_t>(n)));
+    MD_CUDA(s->force2.reserve(3 * static_cast<size_t>(n)));
+    MD_CUDA(s->mass2.reserve(n));
+    MD_CUDA(s->ids2.reserve(n));
+    k_permute<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(d.p, n, s->pos.p, s->vel.p, s->force.p, s->mass.p,
+                                                                   s->ids.p, s->pos2.p, s->vel2.p, s->force2.p,
+                                                                   s->mass2.p, s->ids2.p);
+    MD_CHECK_LAUNCH();
+    k_permute_commit<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(
+        n, d.p, nullptr, s->pos2.p, s->vel2.p, s->force2.p, s->mass2.p, s->ids2.p, s->pos.p, s->vel.p, s->force.p,
+        s->mass.p, s->ids.p, nullptr, nullptr);
+    MD_CHECK_LAUNCH();
+    s->layout++;
+    return sync(s);
+}
+
+md_status md_fcc_lattice(int cells, double a, double* pos4) {
+    if (cells < 0 || (!pos4 && cells > 0)) return fail(MD_ERR_INVALID, "md_fcc_lattice: bad arguments");
+    // src/Initialisation.cpp:7-44: basis atoms of the cubic cell, offset by a quarter cell
+    static constexpr double basis[4][3] = {{0.0, 0.0, 0.0}, {0.5, 0.5, 0.0}, {0.5, 0.0, 0.5}, {0.0, 0.5, 0.5}};
+    size_t p = 0;
+    for (int ix = 0; ix < cells; ++ix)
+        for (int iy = 0; iy < cells; ++iy)
+            for (int iz = 0; iz < cells; ++iz)
+                for (const auto& b : basis) {
+                    pos4[4 * p + 0] = (ix + b[0] + 0.25) * a;
+                    pos4[4 * p + 1] = (iy + b[1] + 0.25) * a;
+                    pos4[4 * p + 2] = (iz + b[2] + 0.25) * a;
+                    pos4[4 * p + 3] = 0.0;
+                    ++p;
+                }
+    return MD_OK;
+}
+
+md_status md_initialize_velocities(md_system* s, double temperature, uint32_t seed) {
+    if (!s) return fail(MD_ERR_INVALID, "null system");
+    const size_t n = static_cast<size_t>(s->n);
+    std::vector<double> mass(n), vel(3 * n);
+    MD_TRY(md_system_download(s, nullptr, nullptr, nullptr, mass.data(), nullptr));
+    // src/Initialisation.cpp:47-76: one normal_distribution(0, sqrt(T / m)) per particle, drawn x, y, z
+    std::mt19937 rng(seed);
+    double momentum[3] = {0.0, 0.0, 0.0};
+    double total_mass = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        std::normal_distribution<double> dist(0.0, std::sqrt(temperature / mass[i]));
+        for (int k = 0; k < 3; ++k) {
+            const double v = dist(rng);
+            vel[k * n + i] = v;
+            momentum[k] += mass[i] * v;
+        }
+        total_mass += mass[i];
+    }
+    for (int k = 0; k < 3; ++k)
+        for (size_t i = 0; i < n; ++i) vel[k * n + i] -= momentum[k] / total_mass;
+    MD_TRY(md_system_upload(s, nullptr, vel.data(), nullptr, nullptr, nullptr));
+    return md_rescale_velocities(s, temperature);
+}
+
+md_status md_system_stream(md_system* s, void** stream) {
+    if (!s || !stream) return fail(MD_ERR_INVALID, "md_system_stream: bad arguments");
+    *stream = s->stream;
+    return MD_OK;
+}
+
+md_status md_system_synchronize(md_system* s) {
+    if (!s) return fail(MD_ERR_INVALID, "null system");
+    MD_TRY(use_system(s));
+    return sync(s);
+}
+
+md_status md_system_launch_count(const md_system* s, uint64_t* launches) {
+    if (!s || !launches) return fail(MD_ERR_INVALID, "md_system_launch_count: bad arguments");
+    *launches = s->launches;
+    return MD_OK;
+}
+
+md_status md_profile_enable(md_system* s, int enable) {
+    if (!s) return fail(MD_ERR_INVALID, "null system");
+    MD_TRY(use_system(s));
+    MD_TRY(sync(s));
+    s->profile = enable != 0;
+    s->events_used = 0;
+    s->profile_ms = 0.0;
+    s->profile_count = 0;
+    return MD_OK;
+}
+
+md_status md_profile_read(md_system* s, double* force_ms, int64_t* force_launches) {
+    if (!s) return fail(MD_ERR_INVALID, "null system");
+    MD_TRY(use_system(s));
+    MD_TRY(sync(s));
+    MD_TRY(profile_collect(s));
+    if (force_ms) *force_ms = s->profile_ms;
+    if (force_launches) *force_launches = s->profile_count;
+    return MD_OK;
+}
+
+md_status md_kinetic_energy(md_system* s, double* out) {
+    if (!s || !out) return fail(MD_ERR_INVALID, "md_kinetic_energy: bad arguments");
+    MD_TRY(use_system(s));
+    MD_TRY(kinetic_async(s));
+    MD_CUDA(cudaMemcpyAsync(s->host_scal, s->scal.p + kScalKE, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    MD_TRY(sync(s));
+    *out = s->host_scal[0];
+    return MD_OK;
+}
+
+md_status md_temperature(md_system* s, double* out) {
+    double ke = 0.0;
+    MD_TRY(md_kinetic_energy(s, &ke));
+    *out = 2.0 * ke / dof_of(s->n);  // src/System.cpp:79-82
+    return MD_OK;
+}
+
+md_status md_state_hash(md_system* s, uint64_t* out) {
+    if (!s || !out) return fail(MD_ERR_INVALID, "md_state_hash: bad arguments");
+    const size_t n = static_cast<size_t>(s->n);
+    std::vector<double> pos(4 * n), vel(3 * n);
+    MD_TRY(md_system_download(s, pos.data(), vel.data(), nullptr, nullptr, nullptr));
+    // FNV-1a over (x, vx, y, vy, z, vz) per particle (src/System.cpp:85-105)
+    uint64_t h = 14695981039346656037ull;
+    auto mix = [&h](double v) {
+        uint64_t bits;
+        std::memcpy(&bits, &v, 8);
+        for (unsigned b = 0; b < 8; ++b) {
+            h ^= (bits >> (8u * b)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    };
+    for (size_t i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            mix(pos[4 * i + k]);
+            mix(vel[k * n + i]);
+        }
+    *out = h;
+    return MD_OK;
+}
+
+md_status md_scale_velocities(md_system* s, double scale) {
+    if (!s) return fail(MD_ERR_INVALID, "null system");
+    MD_TRY(use_system(s));
+    s->host_scal[kScalFactor] = scale;
+    s->host_scal[kScalFactor + 1] = 1.0;
+    MD_CUDA(cudaMemcpyAsync(s->scal.p + kScalFactor, s->host_scal + kScalFactor, 2 * sizeof(double),
+                            cudaMemcpyHostToDevice, s->stream));
+    MD_TRY(scale_async(s));
+    return sync(s);
+}
+
+md_status md_rescale_velocities(md_system* s, double target) {
+    if (!s) return fail(MD_ERR_INVALID, "null system");
+    MD_TRY(use_system(s));
+    MD_TRY(kinetic_async(s));
+    k_rescale_factor<<<1, 1, 0, s->stream>>>(s->scal.p + kScalKE, dof_of(s->n), target, s->scal.p + kScalFactor);
+    MD_CHECK_LAUNCH();
+    MD_TRY(scale_async(s));
+    return sync(s);
+}
+
+md_status md_bussi_apply(md_system* s, double temperature, double tau, double dt, double r1, double chi2) {
+    if (!s) return fail(MD_ERR_INVALID, "null system");
+    MD_TRY(use_system(s));
+    const double c = std::exp(-dt / tau);  // src/Thermostat.cpp:46
+    s->host_scal[kScalR1] = r1;
+    s->host_scal[kScalR1 + 1] = chi2;
+    MD_CUDA(cudaMemcpyAsync(s->scal.p + kScalR1, s->host_scal + kScalR1, 2 * sizeof(double), cudaMemcpyHostToDevice,
+                            s->stream));
+    MD_TRY(kinetic_async(s));
+    k_bussi_factor<<<1, 1, 0, s->stream>>>(s->scal.p + kScalKE, dof_of(s->n), temperature, c, s->scal.p + kScalR1,
+                                           s->scal.p + kScalR1 + 1, s->scal.p + kScalFactor);
+    MD_CHECK_LAUNCH();
+    MD_TRY(scale_async(s));
+    return sync(s);
+}
+
+md_status md_bussi_noise(uint64_t seed, int64_t n, int64_t count, double* r1, double* chi2) {
+    if ((count > 0 && (!r1 || !chi2)) || count < 0 || n < 2) return fail(MD_ERR_INVALID, "md_bussi_noise: bad arguments");
+    std::mt19937_64 rng(seed);
+    const double dof = dof_of(n);
+    for (int64_t k = 0; k < count; ++k) {
+        // fresh distributions per call, as BussiThermostat::apply constructs them (src/Thermostat.cpp:48-51)
+        std::normal_distribution<double> gaussian(0.0, 1.0);
+        std::gamma_distribution<double> gamma(0.5 * (dof - 1.0), 2.0);
+        r1[k] = gaussian(rng);
+        chi2[k] = gamma(rng);
+    }
+    return MD_OK;
+}
+
+// ---- CellList ----------------------------------------------------------------------------------------------
+
+md_status md_cells_create(double min_cell_size, md_cells** out) {
+    if (!out || !(min_cell_size > 0.0)) return fail(MD_ERR_INVALID, "md_cells_create: bad arguments");
+    auto* c = new md_cells;
+    c->min_size = min_cell_size;
+    *out = c;
+    return MD_OK;
+}
+
+md_status md_cells_destroy(md_cells* c) {
+    if (c && c->device >= 0) cudaSetDevice(c->device);
+    delete c;
+    return MD_OK;
+}
+
+md_status md_cells_build(md_cells* c, md_system* s, int* cells_per_side) {
+    if (!c || !s) return fail(MD_ERR_INVALID, "md_cells_build: bad arguments");
+    MD_TRY(use_system(s));
+    c->device = s->device;
+    c->n = s->n;
+    MD_TRY(cell_sort(c->g, s, c->min_size));
+    MD_TRY(sync(s));
+    if (cells_per_side) *cells_per_side = c->g.ncps;
+    return MD_OK;
+}
+
+md_status md_cells_download(md_cells* c, int* particle_cell, uint64_t* cell_start, uint64_t* cell_particles) {
+    if (!c || c->device < 0) return fail(MD_ERR_STATE, "cell list not built");
+    MD_TRY(use_device(c->device));
+    const size_t n = static_cast<size_t>(c->n);
+    if (particle_cell && n) MD_CUDA(cudaMemcpy(particle_cell, c->g.cell_of.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    if (cell_start) {
+        std::vector<int> st(c->g.ncells + 1);
+        MD_CUDA(cudaMemcpy(st.data(), c->g.start.p, sizeof(int) * st.size(), cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < st.size(); ++k) cell_start[k] = static_cast<uint64_t>(st[k]);
+    }
+    if (cell_particles && n) {
+        std::vector<uint32_t> o(n);
+        MD_CUDA(cudaMemcpy(o.data(), c->g.order.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < n; ++k) cell_particles[k] = o[k];
+    }
+    return MD_OK;
+}
+
+// ---- NeighbourList -----------------------------------------------------------------------------------------
+
+md_status md_nlist_create(double cutoff, double skin, int reverse_index, md_nlist** out) {
+    if (!out || !(cutoff > 0.0) || !(skin >= 0.0)) return fail(MD_ERR_INVALID, "md_nlist_create: bad arguments");
+    auto* nl = new md_nlist;
+    // src/NeighbourList.cpp:5-8
+    nl->rc = cutoff;
+    nl->skin = skin;
+    nl->rl = cutoff + skin;
+    nl->rl2 = (cutoff + skin) * (cutoff + skin);
+    nl->max_disp2 = 0.25 * skin * skin;
+    nl->reverse = reverse_index != 0;
+    *out = nl;
+    return MD_OK;
+}
+
+md_status md_nlist_destroy(md_nlist* nl) {
+    if (nl && nl->device >= 0) cudaSetDevice(nl->device);
+    delete nl;
+    return MD_OK;
+}
+
+md_status md_nlist_build(md_nlist* nl, md_system* s) {
+    if (!nl || !s) return fail(MD_ERR_INVALID, "md_nlist_build: bad arguments");
+    MD_TRY(use_system(s));
+    return nlist_build(nl, s);
+}
+
+md_status md_nlist_update(md_nlist* nl, md_system* s, int* rebuilt) {
+    if (!nl || !s) return fail(MD_ERR_INVALID, "md_nlist_update: bad arguments");
+    MD_TRY(use_system(s));
+    bool stale = true;
+    // A list never built for this many particles is stale (src/NeighbourList.cpp:14-18)
+    if (nl->built && nl->n == s->n && nl->sys == s) {
+        const int n = static_cast<int>(s->n);
+        MD_CUDA(cudaMemsetAsync(nl->flags.p, 0, sizeof(int), s->stream));
+        if (n > 0) {
+            k_skin_check<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(s->pos.p, n, s->box, nl->ref_pos.p,
+                                                                              nl->max_disp2, nl->flags.p);
+            MD_CHECK_LAUNCH();
+        }
+        int flag = 0;
+        MD_CUDA(cudaMemcpyAsync(&flag, nl->flags.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        MD_TRY(sync(s));
+        stale = flag != 0;
+    }
+    if (stale) MD_TRY(nlist_build(nl, s));
+    if (rebuilt) *rebuilt = stale ? 1 : 0;
+    return MD_OK;
+}
+
+md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_count, int* cells_per_side,
+                        int* reverse_index) {
+    if (!nl) return fail(MD_ERR_INVALID, "null list");
+    if (pair_count) *pair_count = nl->pairs;
+    if (rebuild_count) *rebuild_count = nl->rebuilds;
+    if (cells_per_side) *cells_per_side = nl->grid.ncps;
+    if (reverse_index) *reverse_index = nl->reverse ? 1 : 0;
+    return MD_OK;
+}
+
+md_status md_nlist_download(md_nlist* nl, uint64_t* offsets, uint64_t* neighbours, uint64_t* rev_offsets,
+                            uint64_t* rev_pairs) {
+    if (!nl) return fail(MD_ERR_INVALID, "null list");
+    if (!nl->built) return fail(MD_ERR_STATE, "neighbour list not built");
+    MD_TRY(use_system(const_cast<md_system*>(nl->sys)));
+    const int n = static_cast<int>(nl->n);
+    cudaStream_t st = nl->sys->stream;
+    const size_t P = nl->pairs;
+    if (offsets) {
+        std::vector<long long> o(n + 1);
+        MD_CUDA(cudaMemcpyAsync(o.data(), nl->half_off.p, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost, st));
+        MD_CUDA(cudaStreamSynchronize(st));
+        for (int i = 0; i <= n; ++i) offsets[i] = static_cast<uint64_t>(o[i]);
+    }
+    if (neighbours && P) {
+        DevBuf<uint64_t> d;
+        MD_CUDA(d.reserve(P));
+        k_half_csr<<<blocks_for(n, kThreads), kThreads, 0, st>>>(nl->rows.p, n, nl->cap, nl->counts.p, nl->half_off.p, d.p);
+        MD_CHECK_LAUNCH();
+        MD_CUDA(cudaMemcpyAsync(neighbours, d.p, sizeof(uint64_t) * P, cudaMemcpyDeviceToHost, st));
+        MD_CUDA(cudaStreamSynchronize(st));
+    }
+    if ((rev_offsets || rev_pairs) && nl->reverse) {
+        MD_CUDA(nl->rev_off.reserve(n + 1));
+        k_rev_counts<<<blocks_for(std::max(n, 1), kThreads), kThreads, 0, st>>>(nl->counts.p, n, nl->tmp_counts.p);
+        MD_CHECK_LAUNCH();
+        exclusive_scan<int, long long>(nl->tmp_counts.p, n, nl->rev_off.p, nl->tiles.p, st);
+        MD_CHECK_SCAN();
+        if (rev_offsets) {
+            std::vector<long long> o(n + 1);
+            MD_CUDA(cudaMemcpyAsync(o.data(), nl->rev_off.p, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost, st));
+            MD_CUDA(cudaStreamSynchronize(st));
+            for (int i = 0; i <= n; ++i) rev_offsets[i] = static_cast<uint64_t>(o[i]);
+        }
+        if (rev_pairs && P) {
+            DevBuf<uint64_t> d;
+            MD_CUDA(d.reserve(P));
+            k_reverse_pairs<<<blocks_for(n, kThreads), kThreads, 0, st>>>(nl->rows.p, n, nl->cap, nl->counts.p,
+                                                                          nl->half_off.p, nl->rev_off.p, d.p);
+            MD_CHECK_LAUNCH();
+            MD_CUDA(cudaMemcpyAsync(rev_pairs, d.p, sizeof(uint64_t) * P, cudaMemcpyDeviceToHost, st));
+            MD_CUDA(cudaStreamSynchronize(st));
+        }
+    }
+    MD_CUDA(cudaGetLastError());
+    return MD_OK;
+}
+
+// ---- LennardJonesForceField --------------------------------------------------------------------------------
+
+md_status md_forcefield_create(double epsilon, double sigma, double cutoff, md_forcefield** out) {
+    if (!out || !(cutoff > 0.0)) return fail(MD_ERR_INVALID, "md_forcefield_create: bad arguments");
+    auto* ff = new md_forcefield;
+    ff->eps = epsilon;
+    ff->sigma = sigma;
+    ff->rc = cutoff;
+    // src/Forcefield.cpp:8-15 and the constant factors of pairTerms (:25-36)
+    const double sr6 = std::pow(sigma / cutoff, 6);
+    const double sr12 = sr6 * sr6;
+    ff->lj.shift = 4.0 * epsilon * (sr12 - sr6);
+    ff->lj.sig2 = sigma * sigma;
+    ff->lj.eps24 = 24.0 * epsilon;
+    ff->lj.eps4 = 4.0 * epsilon;
+    ff->lj.rc2 = cutoff * cutoff;
+    *out = ff;
+    return MD_OK;
+}
+
+md_status md_forcefield_destroy(md_forcefield* ff) {
+    if (ff && ff->device >= 0) cudaSetDevice(ff->device);
+    if (ff && ff->host_out) cudaFreeHost(ff->host_out);
+    delete ff;
+    return MD_OK;
+}
+
+md_status md_forcefield_shift(const md_forcefield* ff, double* shift) {
+    if (!ff || !shift) return fail(MD_ERR_INVALID, "md_forcefield_shift: bad arguments");
+    *shift = ff->lj.shift;
+    return MD_OK;
+}
+
+md_status md_forcefield_set_precision(md_forcefield* ff, int precision) {
+    if (!ff || precision < MD_PREC_FP64 || precision > MD_PREC_FP32) return fail(MD_ERR_INVALID, "bad precision");
+    ff->precision = precision;
+    return MD_OK;
+}
+
+md_status md_forcefield_set_deterministic(md_forcefield* ff, int deterministic) {
+    if (!ff) return fail(MD_ERR_INVALID, "null force field");
+    ff->deterministic = deterministic != 0;
+    return MD_OK;
+}
+
+md_status md_forces_list(md_forcefield* ff, md_system* s, md_nlist* nl, double* pe, double* virial, double* inside) {
+    if (!ff || !s || !nl) return fail(MD_ERR_INVALID, "md_forces_list: bad arguments");
+    MD_TRY(use_system(s));
+    MD_TRY(check_cutoff(ff, s));
+    if (ff->deterministic && !nl->reverse)
+        return fail(MD_ERR_NO_REVERSE_INDEX, "Deterministic forces need a NeighbourList built with reverseIndex = true");
+    if (!nlist_current(nl, s)) return fail(MD_ERR_STATE, "the neighbour list was not built for this system's current order");
+    ff->device = s->device;
+    MD_TRY(forces_list_async(ff, s, nl, true));
+    return read_energy(ff, s, pe, virial, inside);
+}
+
+md_status md_forces_all_pairs(md_forcefield* ff, md_system* s, double* pe, double* virial, double* inside) {
+    if (!ff || !s) return fail(MD_ERR_INVALID, "md_forces_all_pairs: bad arguments");
+    MD_TRY(use_system(s));
+    MD_TRY(check_cutoff(ff, s));
+    ff->device = s->device;
+    const int n = static_cast<int>(s->n);
+    MD_CUDA(ff->out.reserve(4));
+    if (n > 0) {
+        k_force_all_pairs<<<blocks_for(n, 128), 128, 0, s->stream>>>(s->pos.p, n, s->box, ff->lj, s->force.p);
+        MD_CHECK_LAUNCH();
+        k_energy_all_pairs<<<1, 32, 0, s->stream>>>(s->pos.p, n, s->box, ff->lj, ff->out.p);
+        MD_CHECK_LAUNCH();
+    } else {
+        MD_CUDA(cudaMemsetAsync(ff->out.p, 0, 3 * sizeof(double), s->stream));
+    }
+    double out[3];
+    MD_CUDA(cudaMemcpyAsync(out, ff->out.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    MD_TRY(sync(s));
+    ff->virial = out[1];
+    ff->inside = out[2];
+    if (pe) *pe = out[0];
+    if (virial) *virial = out[1];
+    if (inside) *inside = out[2];
+    return MD_OK;
+}
+
+// ---- VelocityVerletIntegrator ------------------------------------------------------------------------------
+
+md_status md_step_list(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, double* pe, int* rebuilt) {
+    if (!s || !ff || !nl) return fail(MD_ERR_INVALID, "md_step_list: bad arguments");
+    MD_TRY(use_system(s));
+    MD_TRY(check_cutoff(ff, s));
+    if (ff->deterministic && !nl->reverse)
+        return fail(MD_ERR_NO_REVERSE_INDEX, "Deterministic forces need a NeighbourList built with reverseIndex = true");
+    ff->device = s->device;
+    const bool current = nlist_current(nl, s);
+    MD_TRY(kick_drift_async(s, nl, dt, current));
+    bool stale = true;
+    if (current) {
+        int flag = 0;
+        MD_CUDA(cudaMemcpyAsync(&flag, nl->flags.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        MD_TRY(sync(s));
+        stale = flag != 0;
+        if (!stale) nl->layout = s->layout;
+    }
+    if (stale) MD_TRY(nlist_build(nl, s));
+    if (rebuilt) *rebuilt = stale ? 1 : 0;
+    MD_TRY(forces_list_async(ff, s, nl, true));
+    MD_TRY(kick_async(s, dt));
+    return read_energy(ff, s, pe, nullptr, nullptr);
+}
+
+md_status md_step_all_pairs(md_system* s, md_forcefield* ff, double dt, double* pe) {
+    if (!s || !ff) return fail(MD_ERR_INVALID, "md_step_all_pairs: bad arguments");
+    MD_TRY(use_system(s));
+    MD_TRY(check_cutoff(ff, s));
+    MD_TRY(kick_drift_async(s, nullptr, dt, false));
+    MD_TRY(md_forces_all_pairs(ff, s, pe, nullptr, nullptr));
+    MD_TRY(kick_async(s, dt));
+    return sync(s);
+}
+
+// ---- RadialDistribution --------------------------------------------------------------------------------------
+
+md_status md_rdf_create(double r_max, int bins, md_rdf** out) {
+    if (!out || !(r_max > 0.0) || bins <= 0 || bins > (1 << 20)) return fail(MD_ERR_INVALID, "md_rdf_create: bad arguments");
+    auto* r = new md_rdf;
+    r->rmax = r_max;
+    r->bins = bins;
+    r->bin_width = r_max / bins;  // src/RadialDistribution.cpp:6-7
+    *out = r;
+    return MD_OK;
+}
+
+md_status md_rdf_destroy(md_rdf* r) {
+    if (r && r->device >= 0) cudaSetDevice(r->device);
+    delete r;
+    return MD_OK;
+}
+
+md_status md_rdf_sample(md_rdf* r, md_system* s, md_nlist* nl) {
+    if (!r || !s || !nl) return fail(MD_ERR_INVALID, "md_rdf_sample: bad arguments");
+    MD_TRY(use_system(s));
+    if (!nlist_current(nl, s)) return fail(MD_ERR_STATE, "the neighbour list was not built for this system's current order");
+    if (r->device >= 0 && r->device != s->device) return fail(MD_ERR_INVALID, "histogram lives on another device");
+    MD_TRY(rdf_sample_async(r, s, nl));
+    return sync(s);
+}
+
+md_status md_rdf_histogram(md_rdf* r, double* hist) {
+    if (!r || !hist) return fail(MD_ERR_INVALID, "md_rdf_histogram: bad arguments");
+    if (r->device < 0) {
+        for (int b = 0; b < r->bins; ++b) hist[b] = 0.0;
+        return MD_OK;
+    }
+    MD_TRY(use_device(r->device));
+    std::vector<unsigned long long> h(r->bins);
+    MD_CUDA(cudaMemcpy(h.data(), r->hist.p, sizeof(unsigned long long) * r->bins, cudaMemcpyDeviceToHost));
+    for (int b = 0; b < r->bins; ++b) hist[b] = static_cast<double>(h[b]);
+    return MD_OK;
+}
+
+md_status md_rdf_values(md_rdf* r, double* radii, double* g, int* samples) {
+    if (!r) return fail(MD_ERR_INVALID, "null rdf");
+    std::vector<double> h(r->bins);
+    MD_TRY(md_rdf_histogram(r, h.data()));
+    for (int b = 0; b < r->bins; ++b) {
+        if (radii) radii[b] = (static_cast<double>(b) + 0.5) * r->bin_width;  // src/RadialDistribution.cpp:32-38
+        if (g) {
+            if (r->samples == 0) {
+                g[b] = 0.0;
+                continue;
+            }
+            // src/RadialDistribution.cpp:42-54
+            const double lo = static_cast<double>(b) * r->bin_width;
+            const double hi = lo + r->bin_width;
+            const double shell = 4.0 / 3.0 * 3.14159265358979323846 * (hi * hi * hi - lo * lo * lo);
+            g[b] = h[b] / (r->samples * 0.5 * r->particles * r->density * shell);
+        }
+    }
+    if (samples) *samples = r->samples;
+    return MD_OK;
+}
+
+// ---- device-resident run -------------------------------------------------------------------------------------
+
+md_status md_run(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps, const md_run_options* opts,
+                 double* pe, double* ke, double* virial) {
+    if (!s || !ff || !nl || n_steps < 0) return fail(MD_ERR_INVALID, "md_run: bad arguments");
+    MD_TRY(use_system(s));
+    MD_TRY(check_cutoff(ff, s));
+    if (ff->deterministic && !nl->reverse)
+        return fail(MD_ERR_NO_REVERSE_INDEX, "Deterministic forces need a NeighbourList built with reverseIndex = true");
+    md_run_options o{};
+    if (opts) o = *opts;
+    if (o.thermostat == 2 && n_steps > 0 && (!o.bussi_r1 || !o.bussi_chi2))
+        return fail(MD_ERR_INVALID, "Bussi run needs r1 and chi2 draws");
+    if (o.thermostat == 1 && o.rescale_every <= 0) return fail(MD_ERR_INVALID, "rescale_every must be positive");
+    if (o.rdf && o.rdf_every <= 0) return fail(MD_ERR_INVALID, "rdf_every must be positive");
+    ff->device = s->device;
+    return run_steps(s, ff, nl, dt, n_steps, o, pe, ke, virial);
+}
+
+}  // extern "C"

@@ -1,0 +1,103 @@
+// Cell list: counting sort of particles into cubic cells, stable in particle index, and the particle reorder
+// that NeighbourList::build performs on every rebuild.
+//
+// Reference: src/CellList.cpp:9-52 (cell id, histogram, prefix sum, stable scatter) and src/System.cpp:42-64
+// (reorder). The stable scatter is done GPU-style: an atomic scatter into each cell's bucket (any order),
+// then one warp per cell ranks its bucket by particle index, which restores the reference's order exactly.
+#pragma once
+
+#include "md_common.cuh"
+
+namespace md {
+
+// std::min(static_cast<int>(x * inverseCellSize), cellsPerSide - 1) (src/CellList.cpp:34). The lower clamp
+// only matters for a coordinate below -1 cell, which the reference does not handle (it would index out of
+// range); it keeps the device in bounds.
+__device__ __forceinline__ int cell_coord(double x, double inv_cell, int ncps) {
+    int c = __double2int_rz(dmul(x, inv_cell));
+    c = c < ncps - 1 ? c : ncps - 1;
+    return c > 0 ? c : 0;
+}
+
+__global__ void k_cell_assign(const double4* __restrict__ pos, int n, double inv_cell, int ncps,
+                              int* __restrict__ cell_of, int* __restrict__ count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 p = pos[i];
+    const int c = (cell_coord(p.x, inv_cell, ncps) * ncps + cell_coord(p.y, inv_cell, ncps)) * ncps +
+                  cell_coord(p.z, inv_cell, ncps);
+    cell_of[i] = c;
+    atomicAdd(&count[c], 1);
+}
+
+// bucket[start[c] + k] for k < count[c] receives the particles of cell c in arbitrary order
+__global__ void k_cell_scatter(const int* __restrict__ cell_of, int n, const int* __restrict__ start,
+                               int* __restrict__ cursor, uint32_t* __restrict__ bucket) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int c = cell_of[i];
+    bucket[start[c] + atomicAdd(&cursor[c], 1)] = static_cast<uint32_t>(i);
+}
+
+// One warp per cell: each particle's rank in its cell is the number of smaller indices in the bucket, so
+// order[] lists every cell's particles in increasing index, as the reference's serial scatter does
+// (src/CellList.cpp:48-51).
+__global__ void k_cell_rank(const int* __restrict__ start, int ncells, const uint32_t* __restrict__ bucket,
+                            uint32_t* __restrict__ order) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= ncells) return;
+    const int s = start[warp];
+    const int m = start[warp + 1] - s;
+    for (int e = lane; e < m; e += 32) {
+        const uint32_t v = bucket[s + e];
+        int rank = 0;
+        for (int f = 0; f < m; ++f) rank += bucket[s + f] < v;
+        order[s + rank] = v;
+    }
+}
+
+// new[k] = old[order[k]] for every per-particle array (src/System.cpp:42-64)
+__global__ void k_permute(const uint32_t* __restrict__ order, int n, const double4* __restrict__ pos,
+                          const double* __restrict__ vel, const double* __restrict__ force,
+                          const double* __restrict__ mass, const uint64_t* __restrict__ ids,
+                          double4* __restrict__ pos2, double* __restrict__ vel2, double* __restrict__ force2,
+                          double* __restrict__ mass2, uint64_t* __restrict__ ids2) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t o = order[k];
+    pos2[k] = pos[o];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        vel2[static_cast<size_t>(c) * n + k] = vel[static_cast<size_t>(c) * n + o];
+        force2[static_cast<size_t>(c) * n + k] = force[static_cast<size_t>(c) * n + o];
+    }
+    mass2[k] = mass[o];
+    ids2[k] = ids[o];
+}
+
+// Copy the permuted arrays back, and give the list its per-particle cell (cell_of of the sorted order) and
+// its reference positions (src/NeighbourList.cpp:129-132).
+__global__ void k_permute_commit(int n, const uint32_t* __restrict__ order, const int* __restrict__ cell_of_old,
+                                 const double4* __restrict__ pos2, const double* __restrict__ vel2,
+                                 const double* __restrict__ force2, const double* __restrict__ mass2,
+                                 const uint64_t* __restrict__ ids2, double4* __restrict__ pos,
+                                 double* __restrict__ vel, double* __restrict__ force, double* __restrict__ mass,
+                                 uint64_t* __restrict__ ids, int* __restrict__ cell_sorted,
+                                 double4* __restrict__ ref_pos) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double4 p = pos2[k];
+    pos[k] = p;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        vel[static_cast<size_t>(c) * n + k] = vel2[static_cast<size_t>(c) * n + k];
+        force[static_cast<size_t>(c) * n + k] = force2[static_cast<size_t>(c) * n + k];
+    }
+    mass[k] = mass2[k];
+    ids[k] = ids2[k];
+    if (cell_sorted) cell_sorted[k] = cell_of_old[order[k]];
+    if (ref_pos) ref_pos[k] = p;
+}
+
+}  // namespace md

@@ -1,0 +1,378 @@
+// Double-precision kernels that reproduce the reference bit for bit: list forces in the deterministic
+// summation order, the blocked energy/virial/kinetic sums, velocity Verlet, the half-skin check, thermostats
+// and the g(r) histogram.
+#pragma once
+
+#include "md_common.cuh"
+
+namespace md {
+
+// ---- forces -----------------------------------------------------------------------------------------
+
+// computeForcesDeterministic's per-particle sum (src/Forcefield.cpp:264-320): particle i adds F(i, j) over
+// its own pairs in list order, then subtracts F(j, i) over the pairs where it is second, in increasing pair
+// index. Pairs outside the cutoff contribute an exact zero in the reference and are skipped here. The
+// inside-cutoff count is the number of own pairs with r^2 < r_c^2 (a sum of whole numbers, exact).
+__global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ lj, const uint32_t* __restrict__ rows,
+                             int cap, const int2* __restrict__ counts, double* __restrict__ force,
+                             unsigned long long* __restrict__ inside) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long ins = 0;
+    if (i < n) {
+        const double4 pi = pos[i];
+        const uint32_t* row = rows + static_cast<size_t>(i) * cap;
+        const int2 c = counts[i];
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (int s = 0; s < c.x; ++s) {
+            const double4 pj = pos[row[s] & kIndexMask];
+            const double dx = min_image(dsub(pi.x, pj.x), box);
+            const double dy = min_image(dsub(pi.y, pj.y), box);
+            const double dz = min_image(dsub(pi.z, pj.z), box);
+            const double r2 = norm2(dx, dy, dz);
+            if (!(r2 < lj.rc2)) continue;
+            double f, e;
+            pair_terms(r2, lj, f, e);
+            fx = dadd(fx, dmul(f, dx));
+            fy = dadd(fy, dmul(f, dy));
+            fz = dadd(fz, dmul(f, dz));
+            ++ins;
+        }
+        for (int s = c.x; s < c.x + c.y; ++s) {
+            const double4 pj = pos[row[s] & kIndexMask];
+            const double dx = min_image(dsub(pj.x, pi.x), box);
+            const double dy = min_image(dsub(pj.y, pi.y), box);
+            const double dz = min_image(dsub(pj.z, pi.z), box);
+            const double r2 = norm2(dx, dy, dz);
+            if (!(r2 < lj.rc2)) continue;
+            double f, e;
+            pair_terms(r2, lj, f, e);
+            fx = dsub(fx, dmul(f, dx));
+            fy = dsub(fy, dmul(f, dy));
+            fz = dsub(fz, dmul(f, dz));
+        }
+        force[i] = fx;
+        force[static_cast<size_t>(n) + i] = fy;
+        force[2 * static_cast<size_t>(n) + i] = fz;
+    }
+    ins = warp_sum_u64(ins);
+    if ((threadIdx.x & 31) == 0 && ins) atomicAdd(inside, ins);
+}
+
+// Energy and virial of pairs [k0, k1) of the half list in the reference's pair order, summed from 0.0 one
+// after another (the inner loop of deterministicSum, include/Parallel.hpp:43-46): pairEnergy[k] = E when
+// r^2 < r_c^2 else 0, pairVirial[k] = (F/r) r^2 likewise (src/Forcefield.cpp:288-296). One warp per
+// 1024-pair block; lanes evaluate pairs into shared memory, lane 0 sums them in order.
+constexpr int kEnergyWarps = 4;
+__global__ void k_energy_blocks_fp64(const double4* __restrict__ pos, int n, Box box, LJ lj,
+                                     const uint32_t* __restrict__ rows, int cap,
+                                     const long long* __restrict__ half_off, long long pairs,
+                                     double2* __restrict__ block_sums, int nblocks) {
+    extern __shared__ double2 sm_ew[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int blk = blockIdx.x * kEnergyWarps + warp;
+    if (blk >= nblocks) return;
+    double2* ew = sm_ew + warp * kChunk;
+    const long long k0 = static_cast<long long>(blk) * kChunk;
+    const long long k1 = k0 + kChunk < pairs ? k0 + kChunk : pairs;
+    // first particle whose pairs reach k0: the last i with half_off[i] <= k0
+    int i = 0;
+    if (lane == 0) {
+        int lo = 0, hi = n;  // half_off[lo] <= k0 < half_off[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (half_off[mid] <= k0) lo = mid; else hi = mid;
+        }
+        i = lo;
+    }
+    i = __shfl_sync(0xffffffffu, i, 0);
+    for (; i < n && half_off[i] < k1; ++i) {
+        const long long b = half_off[i];
+        const long long kb = b > k0 ? b : k0;
+        const long long ke = half_off[i + 1] < k1 ? half_off[i + 1] : k1;
+        const double4 pi = pos[i];
+        const uint32_t* row = rows + static_cast<size_t>(i) * cap;
+        for (long long k = kb + lane; k < ke; k += 32) {
+            const double4 pj = pos[row[k - b] & kIndexMask];
+            const double dx = min_image(dsub(pi.x, pj.x), box);
+            const double dy = min_image(dsub(pi.y, pj.y), box);
+            const double dz = min_image(dsub(pi.z, pj.z), box);
+            const double r2 = norm2(dx, dy, dz);
+            double f, e;
+            pair_terms(r2, lj, f, e);
+            const bool in = r2 < lj.rc2;
+            f = in ? f : 0.0;
+            ew[k - k0] = make_double2(in ? e : 0.0, dmul(f, r2));
+        }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        double se = 0.0, sw = 0.0;
+        const int m = static_cast<int>(k1 - k0);
+        for (int t = 0; t < m; ++t) {
+            const double2 v = ew[t];
+            se = dadd(se, v.x);
+            sw = dadd(sw, v.y);
+        }
+        block_sums[blk] = make_double2(se, sw);
+    }
+}
+
+// The outer loop of deterministicSum (include/Parallel.hpp:52-56): block sums added in order from 0.0.
+// One warp; lanes stage 32 values at a time, lane 0 adds them one after another.
+__global__ void k_sum_blocks(const double2* __restrict__ block_sums, int nblocks, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    double se = 0.0, sw = 0.0;
+    for (int b0 = 0; b0 < nblocks; b0 += 32) {
+        const double2 v = b0 + lane < nblocks ? block_sums[b0 + lane] : make_double2(0.0, 0.0);
+        const int m = nblocks - b0 < 32 ? nblocks - b0 : 32;
+        for (int t = 0; t < m; ++t) {
+            const double x = __shfl_sync(0xffffffffu, v.x, t);
+            const double y = __shfl_sync(0xffffffffu, v.y, t);
+            if (lane == 0) {
+                se = dadd(se, x);
+                sw = dadd(sw, y);
+            }
+        }
+    }
+    if (lane == 0) {
+        out[0] = se;
+        out[1] = sw;
+    }
+}
+
+// ---- kinetic energy -----------------------------------------------------------------------------------
+
+// 0.5 * m * (vx^2 + vy^2 + vz^2) over particles [1024 b, 1024 b + 1024) summed in order (src/System.cpp:67-76)
+__global__ void k_kinetic_blocks(const double* __restrict__ vel, const double* __restrict__ mass, int n,
+                                 double2* __restrict__ block_sums, int nblocks) {
+    extern __shared__ double2 sm_ke[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int blk = blockIdx.x * kEnergyWarps + warp;
+    if (blk >= nblocks) return;
+    double* v = reinterpret_cast<double*>(sm_ke + warp * (kChunk / 2));
+    const int i0 = blk * kChunk;
+    const int m = n - i0 < kChunk ? n - i0 : kChunk;
+    for (int t = lane; t < m; t += 32) {
+        const int i = i0 + t;
+        const double vx = vel[i], vy = vel[static_cast<size_t>(n) + i], vz = vel[2 * static_cast<size_t>(n) + i];
+        v[t] = dmul(dmul(0.5, mass[i]), norm2(vx, vy, vz));
+    }
+    __syncwarp();
+    if (lane == 0) {
+        double s = 0.0;
+        for (int t = 0; t < m; ++t) s = dadd(s, v[t]);
+        block_sums[blk] = make_double2(s, 0.0);
+    }
+}
+
+// ---- integration --------------------------------------------------------------------------------------
+
+// VelocityVerletIntegrator::kickAndDrift (src/Integrator.cpp:32-53): v += (dt/2) f / m, then
+// r = wrap(r + dt v). Fused with NeighbourList::update's staleness test (src/NeighbourList.cpp:24-30) against
+// the reference positions of the last build, which sets *stale when any |d|^2 > skin^2 / 4.
+__global__ void k_kick_drift(double4* __restrict__ pos, double* __restrict__ vel, const double* __restrict__ force,
+                             const double* __restrict__ mass, int n, double half_dt, double dt, Box box,
+                             const double4* __restrict__ ref_pos, double max_disp2, int* __restrict__ stale) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double m = mass[i];
+    double4 p = pos[i];
+    double* pc[3] = {&p.x, &p.y, &p.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const size_t o = static_cast<size_t>(k) * n + i;
+        const double v = dadd(vel[o], ddiv(dmul(half_dt, force[o]), m));
+        vel[o] = v;
+        *pc[k] = wrap(dadd(*pc[k], dmul(dt, v)), box);
+    }
+    pos[i] = p;
+    if (ref_pos) {
+        const double4 r = ref_pos[i];
+        const double dx = min_image(dsub(p.x, r.x), box);
+        const double dy = min_image(dsub(p.y, r.y), box);
+        const double dz = min_image(dsub(p.z, r.z), box);
+        if (norm2(dx, dy, dz) > max_disp2) *stale = 1;
+    }
+}
+
+// NeighbourList::update's test on its own (src/NeighbourList.cpp:24-30)
+__global__ void k_skin_check(const double4* __restrict__ pos, int n, Box box, const double4* __restrict__ ref_pos,
+                             double max_disp2, int* __restrict__ stale) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 p = pos[i], r = ref_pos[i];
+    const double dx = min_image(dsub(p.x, r.x), box);
+    const double dy = min_image(dsub(p.y, r.y), box);
+    const double dz = min_image(dsub(p.z, r.z), box);
+    if (norm2(dx, dy, dz) > max_disp2) *stale = 1;
+}
+
+// VelocityVerletIntegrator::kick (src/Integrator.cpp:55-71)
+__global__ void k_kick(double* __restrict__ vel, const double* __restrict__ force, const double* __restrict__ mass,
+                       int n, double half_dt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double m = mass[i];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const size_t o = static_cast<size_t>(k) * n + i;
+        vel[o] = dadd(vel[o], ddiv(dmul(half_dt, force[o]), m));
+    }
+}
+
+// ---- thermostats ----------------------------------------------------------------------------------------
+
+// Scale factors computed on the device from the device kinetic energy, so no host round trip is needed.
+// scale[0] = factor, scale[1] = 1 to apply or 0 to leave the velocities alone.
+// rescaleVelocities (src/Thermostat.cpp:17-30)
+__global__ void k_rescale_factor(const double* __restrict__ ke, double dof, double target, double* __restrict__ scale) {
+    const double t = ddiv(dmul(2.0, ke[0]), dof);  // System::temperature (src/System.cpp:79-82)
+    if (t <= 0.0) {
+        scale[1] = 0.0;
+        return;
+    }
+    scale[0] = __dsqrt_rn(ddiv(target, t));
+    scale[1] = 1.0;
+}
+
+// BussiThermostat::apply, equation A7 (src/Thermostat.cpp:36-58), with r1 and chi2 given
+__global__ void k_bussi_factor(const double* __restrict__ ke, double dof, double temperature, double c,
+                               const double* __restrict__ r1p, const double* __restrict__ chi2p,
+                               double* __restrict__ scale) {
+    const double kinetic = ke[0];
+    if (kinetic <= 0.0) {
+        scale[1] = 0.0;
+        return;
+    }
+    const double r1 = r1p[0], chi2 = chi2p[0];
+    const double target = dmul(dmul(0.5, dof), temperature);
+    const double omc = dsub(1.0, c);
+    const double t1 = dmul(omc, dsub(ddiv(dmul(target, dadd(chi2, dmul(r1, r1))), dof), kinetic));
+    const double t2 = dmul(dmul(2.0, r1), __dsqrt_rn(dmul(dmul(dmul(ddiv(target, dof), kinetic), omc), c)));
+    const double nk = dadd(dadd(kinetic, t1), t2);
+    scale[0] = __dsqrt_rn(ddiv(nk, kinetic));
+    scale[1] = 1.0;
+}
+
+__global__ void k_scale_velocities(double* __restrict__ vel, long long count, const double* __restrict__ scale) {
+    if (scale[1] == 0.0) return;
+    const double s = scale[0];
+    for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < count;
+         t += static_cast<long long>(gridDim.x) * blockDim.x)
+        vel[t] = dmul(vel[t], s);
+}
+
+// ---- g(r) -------------------------------------------------------------------------------------------------
+
+// RadialDistribution::sample (src/RadialDistribution.cpp:11-30): every half-list pair with r^2 < r_max^2
+// adds one to bin (size_t)(sqrt(r^2) / binWidth). Counts are integers, so atomics keep the result exact.
+// A bin index of `bins` or more (possible only through rounding at r just under r_max) is dropped: the
+// reference would write past its histogram there.
+__global__ void k_rdf_sample(const double4* __restrict__ pos, int n, Box box, const uint32_t* __restrict__ rows,
+                             int cap, const int2* __restrict__ counts, double rmax2, double bin_width, int bins,
+                             unsigned long long* __restrict__ hist) {
+    extern __shared__ unsigned int sm_hist[];
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) sm_hist[b] = 0;
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const double4 pi = pos[i];
+        const uint32_t* row = rows + static_cast<size_t>(i) * cap;
+        const int own = counts[i].x;
+        for (int s = 0; s < own; ++s) {
+            const double4 pj = pos[row[s] & kIndexMask];
+            const double dx = min_image(dsub(pi.x, pj.x), box);
+            const double dy = min_image(dsub(pi.y, pj.y), box);
+            const double dz = min_image(dsub(pi.z, pj.z), box);
+            const double r2 = norm2(dx, dy, dz);
+            if (r2 < rmax2) {
+                const unsigned long long b = __double2ull_rz(ddiv(__dsqrt_rn(r2), bin_width));
+                if (b < static_cast<unsigned long long>(bins)) atomicAdd(&sm_hist[b], 1u);
+            }
+        }
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < bins; b += blockDim.x)
+        if (sm_hist[b]) atomicAdd(&hist[b], static_cast<unsigned long long>(sm_hist[b]));
+}
+
+// ---- O(N^2) forces ----------------------------------------------------------------------------------------
+
+// computeForces(System&) (src/Forcefield.cpp:39-78). Particle p receives, in the reference's loop order,
+// -F(i, p) for i = 0 .. p-1 and then +F(p, j) for j = p+1 .. n-1; pairs at or beyond the cutoff are skipped.
+__global__ void k_force_all_pairs(const double4* __restrict__ pos, int n, Box box, LJ lj, double* __restrict__ force) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const double4 pp = pos[p];
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < n; ++i) {
+        if (i == p) continue;
+        const double4 a = i < p ? pos[i] : pp;
+        const double4 b = i < p ? pp : pos[i];
+        const double dx = min_image(dsub(a.x, b.x), box);
+        const double dy = min_image(dsub(a.y, b.y), box);
+        const double dz = min_image(dsub(a.z, b.z), box);
+        const double r2 = norm2(dx, dy, dz);
+        if (r2 >= lj.rc2) continue;
+        double fr, e;
+        pair_terms(r2, lj, fr, e);
+        if (i < p) {
+            f[0] = dsub(f[0], dmul(fr, dx));
+            f[1] = dsub(f[1], dmul(fr, dy));
+            f[2] = dsub(f[2], dmul(fr, dz));
+        } else {
+            f[0] = dadd(f[0], dmul(fr, dx));
+            f[1] = dadd(f[1], dmul(fr, dy));
+            f[2] = dadd(f[2], dmul(fr, dz));
+        }
+    }
+    force[p] = f[0];
+    force[static_cast<size_t>(n) + p] = f[1];
+    force[2 * static_cast<size_t>(n) + p] = f[2];
+}
+
+// The all-pairs potential, virial and inside count: one sequential sum over pairs (i, j > i) in the
+// reference's loop order, started from 0.0. One warp: lanes evaluate 32 pairs at a time, lane 0 adds them.
+__global__ void k_energy_all_pairs(const double4* __restrict__ pos, int n, Box box, LJ lj, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    double pe = 0.0, w = 0.0, ins = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const double4 pi = pos[i];
+        for (int j0 = i + 1; j0 < n; j0 += 32) {
+            const int j = j0 + lane;
+            double e = 0.0, vir = 0.0;
+            bool in = false;
+            if (j < n) {
+                const double4 pj = pos[j];
+                const double dx = min_image(dsub(pi.x, pj.x), box);
+                const double dy = min_image(dsub(pi.y, pj.y), box);
+                const double dz = min_image(dsub(pi.z, pj.z), box);
+                const double r2 = norm2(dx, dy, dz);
+                if (r2 < lj.rc2) {
+                    double fr;
+                    pair_terms(r2, lj, fr, e);
+                    vir = dmul(fr, r2);
+                    in = true;
+                }
+            }
+            const unsigned mask = __ballot_sync(0xffffffffu, in);
+            const int m = n - j0 < 32 ? n - j0 : 32;
+            for (int t = 0; t < m; ++t) {
+                const double et = __shfl_sync(0xffffffffu, e, t);
+                const double wt = __shfl_sync(0xffffffffu, vir, t);
+                if (lane == 0 && ((mask >> t) & 1u)) {
+                    pe = dadd(pe, et);
+                    w = dadd(w, wt);
+                    ins = dadd(ins, 1.0);
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        out[0] = pe;
+        out[1] = w;
+        out[2] = ins;
+    }
+}
+
+}  // namespace md

@@ -1,0 +1,413 @@
+"""Python mirror of the reference's hot-path classes over libmdgpu.so's C-ABI (include/md_b200.h).
+
+The names and argument meanings follow nhantran1711/molecular-dynamics (include/System.hpp,
+include/CellList.hpp, include/NeighbourList.hpp, include/Forcefield.hpp, include/Integrator.hpp,
+include/Thermostat.hpp, include/RadialDistribution.hpp); the errors the reference throws as
+std::runtime_error are raised as RuntimeError with the same messages. Every computation runs in the CUDA
+library: this module only moves arrays and calls entry points. It raises at import time when the library has
+not been built, and every device call fails loudly when no GPU is present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmdgpu.so")
+
+PREC_FP64, PREC_FP32FX, PREC_FP32 = 0, 1, 2
+_ERRORS = {1: "MD_ERR_INVALID", 2: "MD_ERR_CUTOFF", 3: "MD_ERR_LIST_RADIUS", 4: "MD_ERR_NO_REVERSE_INDEX",
+           5: "MD_ERR_CAPACITY", 6: "MD_ERR_CUDA", 7: "MD_ERR_NO_DEVICE", 8: "MD_ERR_STATE", 9: "MD_ERR_TIMEOUT"}
+
+_P, _D, _I, _I64, _U64 = C.c_void_p, C.c_double, C.c_int, C.c_int64, C.c_uint64
+_PD, _PI, _PU64, _PP = C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_uint64), C.POINTER(C.c_void_p)
+
+
+class MDError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+        self.name = _ERRORS.get(code, str(code))
+
+
+class md_run_options(C.Structure):
+    _fields_ = [("thermostat", C.c_int), ("rescale_every", C.c_int), ("rescale_temperature", C.c_double),
+                ("melt_until", C.c_int), ("melt_temperature", C.c_double), ("bussi_temperature", C.c_double),
+                ("bussi_tau", C.c_double), ("bussi_r1", _PD), ("bussi_chi2", _PD), ("rdf", C.c_void_p),
+                ("rdf_every", C.c_int), ("first_step", C.c_int64)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`")
+    lib = C.CDLL(LIB_PATH)
+    sig = {
+        "md_last_error": (C.c_char_p, []), "md_version": (C.c_char_p, []), "md_device_count": (_I, []),
+        "md_system_create": (_I, [_I64, _D, _I, _PP]), "md_system_destroy": (_I, [_P]),
+        "md_system_size": (_I, [_P, C.POINTER(C.c_int64), _PD]),
+        "md_system_upload": (_I, [_P, _PD, _PD, _PD, _PD, _PU64]),
+        "md_system_download": (_I, [_P, _PD, _PD, _PD, _PD, _PU64]),
+        "md_system_reorder": (_I, [_P, _PU64]), "md_kinetic_energy": (_I, [_P, _PD]),
+        "md_temperature": (_I, [_P, _PD]), "md_state_hash": (_I, [_P, _PU64]),
+        "md_scale_velocities": (_I, [_P, _D]), "md_rescale_velocities": (_I, [_P, _D]),
+        "md_bussi_apply": (_I, [_P, _D, _D, _D, _D, _D]), "md_bussi_noise": (_I, [_U64, _I64, _I64, _PD, _PD]),
+        "md_cells_create": (_I, [_D, _PP]), "md_cells_destroy": (_I, [_P]), "md_cells_build": (_I, [_P, _P, _PI]),
+        "md_cells_download": (_I, [_P, _PI, _PU64, _PU64]),
+        "md_nlist_create": (_I, [_D, _D, _I, _PP]), "md_nlist_destroy": (_I, [_P]),
+        "md_nlist_build": (_I, [_P, _P]), "md_nlist_update": (_I, [_P, _P, _PI]),
+        "md_nlist_info": (_I, [_P, _PU64, _PI, _PI, _PI]),
+        "md_nlist_download": (_I, [_P, _PU64, _PU64, _PU64, _PU64]),
+        "md_forcefield_create": (_I, [_D, _D, _D, _PP]), "md_forcefield_destroy": (_I, [_P]),
+        "md_forcefield_shift": (_I, [_P, _PD]), "md_forcefield_set_precision": (_I, [_P, _I]),
+        "md_forcefield_set_deterministic": (_I, [_P, _I]),
+        "md_forces_list": (_I, [_P, _P, _P, _PD, _PD, _PD]), "md_forces_all_pairs": (_I, [_P, _P, _PD, _PD, _PD]),
+        "md_step_list": (_I, [_P, _P, _P, _D, _PD, _PI]), "md_step_all_pairs": (_I, [_P, _P, _D, _PD]),
+        "md_run": (_I, [_P, _P, _P, _D, _I64, C.POINTER(md_run_options), _PD, _PD, _PD]),
+        "md_rdf_create": (_I, [_D, _I, _PP]), "md_rdf_destroy": (_I, [_P]), "md_rdf_sample": (_I, [_P, _P, _P]),
+        "md_rdf_values": (_I, [_P, _PD, _PD, _PI]), "md_rdf_histogram": (_I, [_P, _PD]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+LIB = _load()
+
+
+def _pd(a):
+    return None if a is None else a.ctypes.data_as(_PD)
+
+
+def _pu(a):
+    return None if a is None else a.ctypes.data_as(_PU64)
+
+
+def _pi(a):
+    return None if a is None else a.ctypes.data_as(_PI)
+
+
+def _check(code: int):
+    if code != 0:
+        raise MDError(code, LIB.md_last_error().decode())
+
+
+def device_count() -> int:
+    return LIB.md_device_count()
+
+
+def bussi_noise(seed: int, n: int, count: int) -> tuple[np.ndarray, np.ndarray]:
+    """The (r1, chi2) draws of `count` successive BussiThermostat::apply calls (src/Thermostat.cpp:48-51)."""
+    r1 = np.zeros(count)
+    chi2 = np.zeros(count)
+    _check(LIB.md_bussi_noise(seed, n, count, _pd(r1), _pd(chi2)))
+    return r1, chi2
+
+
+class System:
+    """System (include/System.hpp:12-136) resident on one GPU. pos is (n, 4): x, y, z, pad; vel/force are
+    (3, n) component arrays, as the reference stores them."""
+
+    def __init__(self, n: int, box_length: float, device: int = 0):
+        h = C.c_void_p()
+        _check(LIB.md_system_create(n, box_length, device, C.byref(h)))
+        self.h = h
+        self.n = n
+        self.box = float(box_length)
+
+    @classmethod
+    def from_arrays(cls, pos, box_length, vel=None, mass=None, force=None, ids=None, device=0) -> "System":
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        if pos.ndim == 2 and pos.shape[1] == 3:
+            pos = np.concatenate([pos, np.zeros((pos.shape[0], 1))], axis=1)
+        s = cls(pos.shape[0], box_length, device)
+        s.upload(pos=pos, vel=vel, mass=mass, force=force, ids=ids)
+        return s
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            LIB.md_system_destroy(h)
+            self.h = None
+
+    def upload(self, pos=None, vel=None, force=None, mass=None, ids=None):
+        def f64(a, shape):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            assert a.size == int(np.prod(shape)), (a.shape, shape)
+            return a
+        pos, vel, force, mass = f64(pos, (self.n, 4)), f64(vel, (3, self.n)), f64(force, (3, self.n)), f64(mass, (self.n,))
+        ids = None if ids is None else np.ascontiguousarray(ids, dtype=np.uint64)
+        _check(LIB.md_system_upload(self.h, _pd(pos), _pd(vel), _pd(force), _pd(mass), _pu(ids)))
+
+    def download(self):
+        pos = np.zeros((self.n, 4))
+        vel = np.zeros((3, self.n))
+        force = np.zeros((3, self.n))
+        mass = np.zeros(self.n)
+        ids = np.zeros(self.n, dtype=np.uint64)
+        _check(LIB.md_system_download(self.h, _pd(pos), _pd(vel), _pd(force), _pd(mass), _pu(ids)))
+        return dict(pos=pos, vel=vel, force=force, mass=mass, ids=ids)
+
+    def positions(self) -> np.ndarray:
+        pos = np.zeros((self.n, 4))
+        _check(LIB.md_system_download(self.h, _pd(pos), None, None, None, None))
+        return pos
+
+    def velocities(self) -> np.ndarray:
+        vel = np.zeros((3, self.n))
+        _check(LIB.md_system_download(self.h, None, _pd(vel), None, None, None))
+        return vel
+
+    def forces(self) -> np.ndarray:
+        f = np.zeros((3, self.n))
+        _check(LIB.md_system_download(self.h, None, None, _pd(f), None, None))
+        return f
+
+    def ids(self) -> np.ndarray:
+        ids = np.zeros(self.n, dtype=np.uint64)
+        _check(LIB.md_system_download(self.h, None, None, None, None, _pu(ids)))
+        return ids
+
+    def reorder(self, order):
+        o = np.ascontiguousarray(order, dtype=np.uint64)
+        _check(LIB.md_system_reorder(self.h, _pu(o)))
+
+    def kinetic_energy(self) -> float:
+        x = C.c_double()
+        _check(LIB.md_kinetic_energy(self.h, C.byref(x)))
+        return x.value
+
+    def temperature(self) -> float:
+        x = C.c_double()
+        _check(LIB.md_temperature(self.h, C.byref(x)))
+        return x.value
+
+    def state_hash(self) -> int:
+        x = C.c_uint64()
+        _check(LIB.md_state_hash(self.h, C.byref(x)))
+        return x.value
+
+    def scale_velocities(self, scale: float):
+        _check(LIB.md_scale_velocities(self.h, scale))
+
+    def rescale_velocities(self, target: float):
+        """rescaleVelocities (src/Thermostat.cpp:17-30)."""
+        _check(LIB.md_rescale_velocities(self.h, target))
+
+    def bussi_apply(self, temperature: float, tau: float, dt: float, r1: float, chi2: float):
+        """BussiThermostat::apply (src/Thermostat.cpp:36-58) with the draws given (see bussi_noise)."""
+        _check(LIB.md_bussi_apply(self.h, temperature, tau, dt, r1, chi2))
+
+
+class CellList:
+    """CellList (include/CellList.hpp:11-50)."""
+
+    def __init__(self, min_cell_size: float):
+        h = C.c_void_p()
+        _check(LIB.md_cells_create(min_cell_size, C.byref(h)))
+        self.h = h
+        self.ncps = 0
+        self.n = 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            LIB.md_cells_destroy(self.h)
+            self.h = None
+
+    def build(self, system: System) -> int:
+        x = C.c_int()
+        _check(LIB.md_cells_build(self.h, system.h, C.byref(x)))
+        self.ncps = x.value
+        self.n = system.n
+        return self.ncps
+
+    def download(self):
+        cell = np.zeros(self.n, dtype=np.int32)
+        start = np.zeros(self.ncps ** 3 + 1, dtype=np.uint64)
+        parts = np.zeros(self.n, dtype=np.uint64)
+        _check(LIB.md_cells_download(self.h, _pi(cell), _pu(start), _pu(parts)))
+        return cell, start, parts
+
+
+class NeighbourList:
+    """NeighbourList (include/NeighbourList.hpp:10-76)."""
+
+    def __init__(self, cutoff: float, skin: float, reverse_index: bool = False):
+        h = C.c_void_p()
+        _check(LIB.md_nlist_create(cutoff, skin, int(reverse_index), C.byref(h)))
+        self.h = h
+        self.reverse_index = reverse_index
+        self.n = 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            LIB.md_nlist_destroy(self.h)
+            self.h = None
+
+    def build(self, system: System):
+        _check(LIB.md_nlist_build(self.h, system.h))
+        self.n = system.n
+
+    def update(self, system: System) -> bool:
+        r = C.c_int()
+        _check(LIB.md_nlist_update(self.h, system.h, C.byref(r)))
+        self.n = system.n
+        return bool(r.value)
+
+    def _info(self):
+        p, rb, nc, rv = C.c_uint64(), C.c_int(), C.c_int(), C.c_int()
+        _check(LIB.md_nlist_info(self.h, C.byref(p), C.byref(rb), C.byref(nc), C.byref(rv)))
+        return p.value, rb.value, nc.value, bool(rv.value)
+
+    @property
+    def pair_count(self) -> int:
+        return self._info()[0]
+
+    @property
+    def rebuild_count(self) -> int:
+        return self._info()[1]
+
+    @property
+    def cells_per_side(self) -> int:
+        return self._info()[2]
+
+    def download(self):
+        P, _, _, rev = self._info()
+        n = self.n
+        off = np.zeros(n + 1, dtype=np.uint64)
+        nb = np.zeros(P, dtype=np.uint64)
+        roff = np.zeros(n + 1, dtype=np.uint64) if rev else None
+        rp = np.zeros(P, dtype=np.uint64) if rev else None
+        _check(LIB.md_nlist_download(self.h, _pu(off), _pu(nb), _pu(roff), _pu(rp)))
+        return dict(offsets=off, neighbours=nb, rev_offsets=roff, rev_pairs=rp)
+
+
+class LennardJonesForceField:
+    """LennardJonesForceField (include/Forcefield.hpp:6-78)."""
+
+    def __init__(self, epsilon: float, sigma: float, cutoff: float, precision: int = PREC_FP64):
+        h = C.c_void_p()
+        _check(LIB.md_forcefield_create(epsilon, sigma, cutoff, C.byref(h)))
+        self.h = h
+        self.virial = 0.0
+        self.inside_pairs = 0.0
+        self.set_precision(precision)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            LIB.md_forcefield_destroy(self.h)
+            self.h = None
+
+    @property
+    def energy_shift(self) -> float:
+        x = C.c_double()
+        _check(LIB.md_forcefield_shift(self.h, C.byref(x)))
+        return x.value
+
+    def set_precision(self, precision: int):
+        _check(LIB.md_forcefield_set_precision(self.h, precision))
+
+    def set_mixed_precision(self, mixed: bool):
+        """setMixedPrecision (include/Forcefield.hpp:39-41): float pair arithmetic, fixed-point accumulation."""
+        self.set_precision(PREC_FP32FX if mixed else PREC_FP64)
+
+    def set_deterministic(self, deterministic: bool):
+        _check(LIB.md_forcefield_set_deterministic(self.h, int(deterministic)))
+
+    def compute_forces(self, system: System, neighbour_list: NeighbourList | None = None) -> float:
+        pe, w, ins = C.c_double(), C.c_double(), C.c_double()
+        if neighbour_list is None:
+            _check(LIB.md_forces_all_pairs(self.h, system.h, C.byref(pe), C.byref(w), C.byref(ins)))
+        else:
+            _check(LIB.md_forces_list(self.h, system.h, neighbour_list.h, C.byref(pe), C.byref(w), C.byref(ins)))
+        self.virial, self.inside_pairs = w.value, ins.value
+        return pe.value
+
+
+class RadialDistribution:
+    """RadialDistribution (include/RadialDistribution.hpp:8-29)."""
+
+    def __init__(self, r_max: float, bins: int):
+        h = C.c_void_p()
+        _check(LIB.md_rdf_create(r_max, bins, C.byref(h)))
+        self.h = h
+        self.bins = bins
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            LIB.md_rdf_destroy(self.h)
+            self.h = None
+
+    def sample(self, system: System, neighbour_list: NeighbourList):
+        _check(LIB.md_rdf_sample(self.h, system.h, neighbour_list.h))
+
+    def radii(self) -> np.ndarray:
+        r = np.zeros(self.bins)
+        _check(LIB.md_rdf_values(self.h, _pd(r), None, None))
+        return r
+
+    def values(self) -> np.ndarray:
+        g = np.zeros(self.bins)
+        _check(LIB.md_rdf_values(self.h, None, _pd(g), None))
+        return g
+
+    def histogram(self) -> np.ndarray:
+        h = np.zeros(self.bins)
+        _check(LIB.md_rdf_histogram(self.h, _pd(h)))
+        return h
+
+
+class VelocityVerletIntegrator:
+    """VelocityVerletIntegrator (include/Integrator.hpp:7-29)."""
+
+    def __init__(self, dt: float):
+        self.dt = dt
+        self.last_rebuilt = False
+
+    def step(self, system: System, force_field: LennardJonesForceField,
+             neighbour_list: NeighbourList | None = None) -> float:
+        pe = C.c_double()
+        if neighbour_list is None:
+            _check(LIB.md_step_all_pairs(system.h, force_field.h, self.dt, C.byref(pe)))
+        else:
+            r = C.c_int()
+            _check(LIB.md_step_list(system.h, force_field.h, neighbour_list.h, self.dt, C.byref(pe), C.byref(r)))
+            self.last_rebuilt = bool(r.value)
+            neighbour_list.n = system.n
+        return pe.value
+
+    def run(self, system: System, force_field: LennardJonesForceField, neighbour_list: NeighbourList, n_steps: int,
+            thermostat: str = "none", rescale_every: int = 10, rescale_temperature: float = 0.0,
+            melt_until: int = 0, melt_temperature: float = 2.0, bussi_temperature: float = 0.0,
+            bussi_tau: float = 0.5, bussi_r1=None, bussi_chi2=None, rdf: RadialDistribution | None = None,
+            rdf_every: int = 10, first_step: int = 1, record: bool = True):
+        """n_steps device-resident steps (md_run). Returns per-step (pe, ke, virial) arrays when record."""
+        o = md_run_options()
+        o.thermostat = {"none": 0, "rescale": 1, "bussi": 2}[thermostat]
+        o.rescale_every = rescale_every
+        o.rescale_temperature = rescale_temperature
+        o.melt_until = melt_until
+        o.melt_temperature = melt_temperature
+        o.bussi_temperature = bussi_temperature
+        o.bussi_tau = bussi_tau
+        keep = []
+        if thermostat == "bussi":
+            r1 = np.ascontiguousarray(bussi_r1, dtype=np.float64)
+            chi2 = np.ascontiguousarray(bussi_chi2, dtype=np.float64)
+            keep += [r1, chi2]
+            o.bussi_r1, o.bussi_chi2 = _pd(r1), _pd(chi2)
+        o.rdf = rdf.h if rdf is not None else None
+        o.rdf_every = rdf_every
+        o.first_step = first_step
+        pe = np.zeros(n_steps) if record else None
+        ke = np.zeros(n_steps) if record else None
+        w = np.zeros(n_steps) if record else None
+        _check(LIB.md_run(system.h, force_field.h, neighbour_list.h, self.dt, n_steps, C.byref(o), _pd(pe), _pd(ke),
+                          _pd(w)))
+        neighbour_list.n = system.n
+        return pe, ke, w

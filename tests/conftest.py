@@ -8,14 +8,15 @@ import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "molecular-dynamics_b200")
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-if ROOT not in sys.path:
-    sys.path.insert(0, ROOT)
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
 
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (sm_100a) and the built libmdgpu.so")
-    config.addinivalue_line("markers", "slow: long-running parity case")
 
 
 @pytest.fixture(scope="session")
@@ -35,7 +36,10 @@ def golden():
 
 @pytest.fixture(scope="session")
 def md():
-    """The product: libmdgpu.so through its C-ABI (ctypes). Fails loudly when the library or GPU is missing."""
-    from md_b200_loader import load_package
+    """The product through its C-ABI (ctypes over libmdgpu.so). Fails, never skips, when the library or the
+    GPU is missing: a GPU test must not pass on a fallback."""
+    import mdgpu
 
-    return load_package()
+    if mdgpu.device_count() < 1:
+        raise RuntimeError("no CUDA device visible to libmdgpu")
+    return mdgpu
