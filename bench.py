@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Throughput of the Lennard-Jones hot path on B200: atom-steps/s of NVE velocity-Verlet steps (cell list,
+neighbour list at its natural rebuild rate, LJ forces, integration) on the 4,000,000-atom FCC fluid.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (the large single system of the benchmark): FCC 100^3 x 4 = 4,000,000 atoms, density 0.8442,
+T* = 0.71 after a 200-step rescale equilibration from a T = 2 melt (md_sim's --melt schedule), r_c = 2.5
+truncated and shifted, skin 0.3, dt 0.005, NVE. The headline precision is FP32 pair arithmetic with 64-bit
+fixed-point force accumulation; the FP64 path (bit-identical to the reference's deterministic mode) is timed
+beside it on the same state. Inputs are synthetic (seeded lattice and velocities) and the working set
+(~1.4 GB) is far larger than the 126 MB L2.
+
+One rank per GPU (torchrun); ranks run independent replicas (seed 42 + rank), so scaling is weak and no
+collective touches the data path. `value` is atom-steps/s summed over ranks, timed with CUDA events on the
+library's stream and taken as the max over ranks.
+
+--impl reference times the reference's own OpenMP CPU code (compiled from its sources into oracle/_ref) on
+this host's cores for a bounded sample of the same workload; rank 0 alone runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "molecular-dynamics_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "atom-steps/s at N=4M, FP32+fixed-pt vs FP64 GPU at <=1e-6 rel force err; %roofline"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def args_parse():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2000)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--cells", type=int, default=100, help="FCC cells per side (N = 4 cells^3)")
+    p.add_argument("--density", type=float, default=0.8442)
+    p.add_argument("--temperature", type=float, default=0.71)
+    p.add_argument("--equil", type=int, default=200)
+    p.add_argument("--precision", choices=["fp32fx", "fp32", "fp64"], default="fp32fx")
+    p.add_argument("--fp64-steps", type=int, default=100, help="steps of the FP64 comparison run (0: skip)")
+    p.add_argument("--cpu-steps", type=int, default=3, help="reference steps in the cpu_baseline sample (0: skip)")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--profile-region", action="store_true",
+                   help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    return p.parse_args()
+
+
+def workload(a) -> dict:
+    n = 4 * a.cells ** 3
+    return {"workload": f"lj_fcc{a.cells}_n{n}_rho{a.density}_T{a.temperature}_rc2.5_skin0.3_dt0.005_nve",
+            "n_atoms": n, "density": a.density, "temperature": a.temperature, "cutoff": 2.5, "skin": 0.3,
+            "dt": 0.005, "equilibration": f"{a.equil} steps, rescale every 10 to T=2 then T={a.temperature}",
+            "precision": a.precision, "l2": "inputs larger than L2 (no flush needed)"}
+
+
+# ---- reference CPU path --------------------------------------------------------------------------------------
+
+def reference_sample(a, steps: int, warmup: int) -> dict:
+    """Time the reference's OpenMP path (oracle/_ref, compiled from its own sources) on all host cores: the
+    same FCC start, list build and list forces, then `warmup` untimed and `steps` timed NVE steps (default
+    force path, as md_sim runs without --deterministic)."""
+    from oracle.oracle import REF_SO, Oracle, Reference, RForceField, RNeighbourList
+
+    threads = os.cpu_count() or 1
+    if os.path.exists(REF_SO):
+        r = Reference()
+        r.set_threads(threads)
+        t0 = time.perf_counter()
+        s = r.fcc_system(a.cells, a.density, a.temperature, 42)
+        nl = RNeighbourList(r, 2.5, 0.3)
+        nl.build(s)
+        ff = RForceField(r, 1.0, 1.0, 2.5)
+        ff.forces(s, nl)
+        setup = time.perf_counter() - t0
+        if warmup:
+            ff.run(s, nl, 0.005, warmup)
+        rb0 = nl.rebuilds
+        t0 = time.perf_counter()
+        ff.run(s, nl, 0.005, steps)
+        dt = time.perf_counter() - t0
+        kind, cores, rebuilds = "reference", r.max_threads(), nl.rebuilds - rb0
+    else:  # the oracle's serial restatement, when the reference could not be built on this machine
+        from oracle.oracle import MODE_DEFAULT, OForceField, ONeighbourList
+        o = Oracle()
+        t0 = time.perf_counter()
+        s = o.fcc_system(a.cells, a.density, a.temperature, 42)
+        nl = ONeighbourList(o, 2.5, 0.3)
+        nl.build(s)
+        ff = OForceField(o, 1.0, 1.0, 2.5)
+        ff.forces(s, nl, MODE_DEFAULT)
+        setup = time.perf_counter() - t0
+        for _ in range(warmup):
+            ff.step(s, nl, 0.005, MODE_DEFAULT)
+        rb0 = nl.rebuilds
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            ff.step(s, nl, 0.005, MODE_DEFAULT)
+        dt = time.perf_counter() - t0
+        kind, cores, rebuilds = "port", 1, nl.rebuilds - rb0
+    n = 4 * a.cells ** 3
+    return {"value": n * steps / dt, "unit": "atom-steps/s", "cores": cores, "kind": kind,
+            "sample": f"{steps} timed NVE steps (after {warmup} untimed) of the same {n}-atom FCC start, "
+                      f"list start, FP64 default force path, {rebuilds} list rebuilds inside the sample; "
+                      f"setup {setup:.1f} s untimed",
+            "ms_per_step": 1e3 * dt / steps, "steps": steps}
+
+
+def run_reference_arm(a):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return  # rank 0 alone runs the CPU reference
+    steps = max(1, min(a.steps, 5))
+    warm = min(a.warmup, 2)
+    cb = reference_sample(a, steps, warm)
+    line = {"metric": METRIC, "value": cb["value"], "unit": "atom-steps/s", "impl": "reference",
+            "n_gpus": a.gpus, "steps": steps, "warmup": warm, "ms_per_step": cb["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload(a),
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---- clocks ------------------------------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi every 200 ms on one GPU during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self) -> dict:
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip() == "Active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---- GPU arm ------------------------------------------------------------------------------------------------
+
+def measured_peak():
+    for path in (os.path.join(ROOT, "MEASURED_PEAKS.json"), "/root/repo/MEASURED_PEAKS.json"):
+        try:
+            with open(path) as f:
+                return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, copy)"
+        except (OSError, KeyError, ValueError):
+            continue
+    return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+def ncu_traffic_per_atom():
+    """DRAM bytes per atom of the force kernel from the committed ncu summary, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "force_fp32fx_traffic.json")) as f:
+            d = json.load(f)
+        return float(d["dram_bytes_per_launch"]) / float(d["n_atoms"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def force_errors(md, s, nl) -> dict:
+    """Per-particle force error of the float modes against the FP64 path on the same state."""
+    import numpy as np
+
+    ff64 = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=md.PREC_FP64)
+    pe64 = ff64.compute_forces(s, nl)
+    w64 = ff64.virial
+    f64 = s.forces()
+    out = {}
+    for name, prec in (("fp32fx", md.PREC_FP32FX), ("fp32", md.PREC_FP32)):
+        ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)
+        pe = ff.compute_forces(s, nl)
+        f = s.forces()
+        d = np.linalg.norm(f - f64, axis=0)
+        mag = np.linalg.norm(f64, axis=0)
+        rel = d / np.maximum(mag, 1e-300)
+        out[name] = {"max_abs_dF_over_max_F": float(np.abs(f - f64).max() / np.abs(f64).max()),
+                     "rms_dF_over_rms_F": float(np.sqrt((d ** 2).mean() / (mag ** 2).mean())),
+                     "per_particle_rel_p50": float(np.percentile(rel, 50)),
+                     "per_particle_rel_p99": float(np.percentile(rel, 99)),
+                     "per_particle_rel_max": float(rel.max()),
+                     "frac_particles_rel_le_1e-6": float((rel <= 1e-6).mean()),
+                     "pe_rel": float(abs(pe - pe64) / abs(pe64)), "virial_rel": float(abs(ff.virial - w64) / abs(w64))}
+    ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=md.PREC_FP32FX)
+    ff.compute_forces(s, nl)
+    return out
+
+
+def run_gpu_arm(a):
+    import numpy as np
+    import torch
+
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    import mdgpu as md
+
+    prec = {"fp32fx": md.PREC_FP32FX, "fp32": md.PREC_FP32, "fp64": md.PREC_FP64}[a.precision]
+    n = 4 * a.cells ** 3
+    dt = 0.005
+    s = md.fcc_system(a.cells, a.density, a.temperature, seed=42 + rank, device=local)
+    nl = md.NeighbourList(2.5, 0.3)
+    ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)
+    integ = md.VelocityVerletIntegrator(dt)
+    nl.build(s)
+    ff.compute_forces(s, nl)
+    if a.equil:
+        integ.run(s, ff, nl, a.equil, thermostat="rescale", rescale_every=10, rescale_temperature=a.temperature,
+                  melt_until=a.equil // 3, melt_temperature=2.0, record=False)
+    errors = force_errors(md, s, nl) if rank == 0 else None
+    if a.warmup:
+        integ.run(s, ff, nl, a.warmup, first_step=a.equil + 1)
+
+    stream = torch.cuda.ExternalStream(s.stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    s.synchronize()
+    rb0, l0 = nl.rebuild_count, s.launch_count
+    s.profile(True)
+    if a.profile_region:
+        torch.cuda.profiler.start()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        pe, ke, _ = integ.run(s, ff, nl, a.steps, first_step=a.equil + a.warmup + 1)
+        ev1.record(stream)
+        ev1.synchronize()
+    if a.profile_region:
+        torch.cuda.profiler.stop()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    force_ms, force_n = s.profile_read()
+    s.profile(False)
+    launches = s.launch_count - l0
+    rebuilds = nl.rebuild_count - rb0
+    pairs = nl.pair_count
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    e0 = pe[0] + ke[0]
+    drift = float(np.abs((pe + ke - e0) / e0).max())
+
+    # FP64 path on a copy of the same state (bit-identical to the reference's deterministic mode)
+    fp64 = None
+    if a.fp64_steps and rank == 0:
+        st = s.download()
+        s64 = md.System.from_arrays(st["pos"], s.box, vel=st["vel"], force=st["force"], device=local)
+        nl64 = md.NeighbourList(2.5, 0.3)
+        nl64.build(s64)
+        ff64 = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=md.PREC_FP64)
+        ff64.compute_forces(s64, nl64)
+        integ.run(s64, ff64, nl64, 5)
+        st64 = torch.cuda.ExternalStream(s64.stream)
+        e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s64.synchronize()
+        s64.profile(True)
+        e0_.record(st64)
+        pe64, ke64, _ = integ.run(s64, ff64, nl64, a.fp64_steps)
+        e1_.record(st64)
+        e1_.synchronize()
+        ms64 = e0_.elapsed_time(e1_)
+        f64_ms, f64_n = s64.profile_read()
+        fp64 = {"value": n * a.fp64_steps / (ms64 / 1e3), "steps": a.fp64_steps, "ms_per_step": ms64 / a.fp64_steps,
+                "force_kernel_ms": f64_ms / max(f64_n, 1),
+                "max_drift": float(np.abs((pe64 + ke64 - pe64[0] - ke64[0]) / (pe64[0] + ke64[0])).max())}
+        del s64, nl64, ff64
+
+    # End to end through the public C-ABI with host buffers: pinned host state -> device, list build,
+    # initial forces, K steps returning per-step PE/KE/virial, final positions and velocities -> host.
+    e2e = None
+    if not a.no_e2e:
+        st = s.download()
+        h_pos = torch.empty((n, 4), dtype=torch.float64, pin_memory=True)
+        h_vel = torch.empty((3, n), dtype=torch.float64, pin_memory=True)
+        h_mass = torch.empty((n,), dtype=torch.float64, pin_memory=True)
+        h_pos.numpy()[:] = st["pos"]
+        h_vel.numpy()[:] = st["vel"]
+        h_mass.numpy()[:] = st["mass"]
+        out_pos = torch.empty((n, 4), dtype=torch.float64, pin_memory=True)
+        out_vel = torch.empty((3, n), dtype=torch.float64, pin_memory=True)
+        s2 = md.System(n, s.box, device=local)
+        nl2 = md.NeighbourList(2.5, 0.3)
+        ff2 = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)
+        st2 = torch.cuda.ExternalStream(s2.stream)
+        x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        s2.synchronize()
+        x0.record(st2)
+        s2.upload(pos=h_pos.numpy(), vel=h_vel.numpy(), mass=h_mass.numpy())
+        nl2.build(s2)
+        ff2.compute_forces(s2, nl2)
+        pe2, ke2, w2 = integ.run(s2, ff2, nl2, a.steps)
+        import ctypes
+        md._check(md.LIB.md_system_download(s2.h, ctypes.cast(out_pos.data_ptr(), md._PD),
+                                            ctypes.cast(out_vel.data_ptr(), md._PD), None, None, None))
+        x1.record(st2)
+        x1.synchronize()
+        ems = x0.elapsed_time(x1)
+        if dist:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        h2d = n * (32 + 24 + 8)
+        d2h = n * (32 + 24) + a.steps * 3 * 8
+        e2e = {"value": world * n * a.steps / (ems / 1e3), "unit": "atom-steps/s",
+               "h2d_bytes_per_step": h2d / a.steps, "d2h_bytes_per_step": d2h / a.steps,
+               "includes": "pinned H2D of positions/velocities/masses, list build, initial forces, all steps with "
+                           "per-step PE/KE/virial read back, D2H of final positions/velocities"}
+        del s2, nl2, ff2
+
+    cpu = None
+    if rank == 0 and world == 1 and a.cpu_steps > 0:
+        cb = reference_sample(a, a.cpu_steps, 1)
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peak, peak_src = measured_peak()
+    kernel_s = (force_ms / max(force_n, 1)) / 1e3
+    bytes_per_atom = 16 + 24 + 4 * 2 * pairs / n  # own float4, fixed-point force, full-list int32 indices
+    achieved = bytes_per_atom * n / kernel_s / 1e9
+    tpa = ncu_traffic_per_atom()
+    value = world * n * a.steps / (ms / 1e3)
+    line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"fp32fx": "f32+i64", "fp32": "f32", "fp64": "f64"}[a.precision],
+            "data": "synthetic", "config": workload(a),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None if tpa is None else tpa * n,
+                         "kernel": "k_force_fp32", "kernel_ms": kernel_s * 1e3,
+                         "algorithmic_bytes_per_atom": bytes_per_atom, "peak_source": peak_src},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+            "rebuilds": rebuilds, "half_list_pairs": pairs, "max_energy_drift": drift,
+            "fp64": fp64, "speedup_vs_fp64": None if fp64 is None else value / world / fp64["value"],
+            "force_error_vs_fp64": errors}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    a = args_parse()
+    if a.impl == "reference":
+        run_reference_arm(a)
+    else:
+        run_gpu_arm(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -67,6 +67,10 @@ def _load():
         "md_run": (_I, [_P, _P, _P, _D, _I64, C.POINTER(md_run_options), _PD, _PD, _PD]),
         "md_rdf_create": (_I, [_D, _I, _PP]), "md_rdf_destroy": (_I, [_P]), "md_rdf_sample": (_I, [_P, _P, _P]),
         "md_rdf_values": (_I, [_P, _PD, _PD, _PI]), "md_rdf_histogram": (_I, [_P, _PD]),
+        "md_fcc_lattice": (_I, [_I, _D, _PD]), "md_initialize_velocities": (_I, [_P, _D, C.c_uint32]),
+        "md_system_stream": (_I, [_P, _PP]), "md_system_synchronize": (_I, [_P]),
+        "md_system_launch_count": (_I, [_P, _PU64]), "md_profile_enable": (_I, [_P, _I]),
+        "md_profile_read": (_I, [_P, _PD, C.POINTER(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -105,6 +109,28 @@ def bussi_noise(seed: int, n: int, count: int) -> tuple[np.ndarray, np.ndarray]:
     chi2 = np.zeros(count)
     _check(LIB.md_bussi_noise(seed, n, count, _pd(r1), _pd(chi2)))
     return r1, chi2
+
+
+def lattice_constant(density: float) -> float:
+    """a = cbrt(4 / density), the FCC lattice constant md_sim uses (src/main.cpp:164-166)."""
+    import math
+
+    return math.cbrt(4.0 / density)
+
+
+def fcc_lattice(cells: int, lattice_constant: float) -> np.ndarray:
+    """createFCCLattice (src/Initialisation.cpp:7-44): (4 cells^3, 4) packed positions."""
+    pos = np.zeros((4 * cells ** 3, 4))
+    _check(LIB.md_fcc_lattice(cells, lattice_constant, _pd(pos)))
+    return pos
+
+
+def fcc_system(cells: int, density: float, temperature: float, seed: int = 42, device: int = 0) -> "System":
+    """The FCC lattice of md_sim with seeded Maxwell-Boltzmann velocities (src/main.cpp:164-170)."""
+    a = lattice_constant(density)
+    s = System.from_arrays(fcc_lattice(cells, a), cells * a, device=device)
+    s.initialize_velocities(temperature, seed)
+    return s
 
 
 class System:
@@ -198,6 +224,35 @@ class System:
     def rescale_velocities(self, target: float):
         """rescaleVelocities (src/Thermostat.cpp:17-30)."""
         _check(LIB.md_rescale_velocities(self.h, target))
+
+    def initialize_velocities(self, temperature: float, seed: int):
+        """initializeVelocities (src/Initialisation.cpp:47-76)."""
+        _check(LIB.md_initialize_velocities(self.h, temperature, seed))
+
+    @property
+    def stream(self) -> int:
+        """The cudaStream_t (as an integer) all of this system's work is queued on."""
+        p = C.c_void_p()
+        _check(LIB.md_system_stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def synchronize(self):
+        _check(LIB.md_system_synchronize(self.h))
+
+    @property
+    def launch_count(self) -> int:
+        x = C.c_uint64()
+        _check(LIB.md_system_launch_count(self.h, C.byref(x)))
+        return x.value
+
+    def profile(self, enable: bool):
+        _check(LIB.md_profile_enable(self.h, int(enable)))
+
+    def profile_read(self) -> tuple[float, int]:
+        """(total ms, launches) of the list force kernel since profile(True)."""
+        ms, k = C.c_double(), C.c_int64()
+        _check(LIB.md_profile_read(self.h, C.byref(ms), C.byref(k)))
+        return ms.value, k.value
 
     def bussi_apply(self, temperature: float, tau: float, dt: float, r1: float, chi2: float):
         """BussiThermostat::apply (src/Thermostat.cpp:36-58) with the draws given (see bussi_noise)."""
