@@ -93,6 +93,19 @@ md_status md_fcc_lattice(int cells, double lattice_constant, double* pos4);
  * host, centre-of-mass removal, then rescaleVelocities on the device. Uses the system's masses. */
 md_status md_initialize_velocities(md_system* s, double temperature, uint32_t seed);
 
+/* Kinetic energy for callers that may not allocate device memory. No counterpart in the reference: it
+ * serves hosts that own all device memory themselves (an embedding runtime with its own pool, or a process
+ * that must not call cudaMalloc/cudaFree while running). vel3 (3 x n, component-major), mass (n) and out (one
+ * double) are device pointers the caller owns; the result is bit-identical to md_kinetic_energy's (same
+ * 1024-particle blocked order). Work is queued on `stream` (a cudaStream_t; NULL = legacy default stream)
+ * and the call returns without waiting. Scratch lives in a fixed 256 KB device array that every GPU loading
+ * the library keeps until exit; n above 16,777,216 is rejected with MD_ERR_INVALID. The first call on a
+ * device looks that array up on the current device (cudaGetSymbolAddress), so make the first call on each
+ * device before any stream capture. All calls share the one array: calls that overlap on the GPU (on
+ * different streams, or from different host threads) race and must be serialised by the caller. The
+ * current device must be the one holding the pointers. No allocating call is made. */
+md_status md_kinetic_energy_noalloc(const double* vel3, const double* mass, int64_t n, double* out, void* stream);
+
 /* ---- streams, timing and counters ---------------------------------------------------------------------- */
 /* The cudaStream_t every call on this system is queued on (for CUDA events around calls). */
 md_status md_system_stream(md_system* s, void** stream);

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <string>
 #include <vector>
@@ -1108,3 +1109,64 @@ md_status md_run(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64
 }
 
 }  // extern "C"
+
+// ---- kinetic energy without allocation ---------------------------------------------------------------------
+//
+// For callers that own every byte of device memory themselves and may not allocate: an embedding runtime
+// with its own pool, or a process that must not call cudaMalloc/cudaFree once running. The block partial
+// sums live in this fixed array instead of an allocation. Every GPU that loads the library holds it (256 KB)
+// until the process exits.
+namespace {
+
+constexpr int64_t kNoAllocMaxBlocks = 16384;  // 1024-particle blocks: up to 16,777,216 particles
+// kNoAllocMaxBlocks block partials, then one slot for the result
+static __device__ __align__(256) double2 g_noalloc_ke_blocks[kNoAllocMaxBlocks + 1];
+
+// Host code must not take g_noalloc_ke_blocks' address directly (it names a host-side shadow): the device
+// address comes from cudaGetSymbolAddress, once per device, with that device current.
+constexpr int kNoAllocMaxDevices = 64;
+double2* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+
+md_status noalloc_scratch(int device, double2** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices) return fail(MD_ERR_INVALID, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        MD_CUDA(cudaGetSymbolAddress(&p, g_noalloc_ke_blocks));
+        g_noalloc_ptr[device] = static_cast<double2*>(p);
+    }
+    *out = g_noalloc_ptr[device];
+    return MD_OK;
+}
+
+}  // namespace
+
+extern "C" md_status md_kinetic_energy_noalloc(const double* vel3, const double* mass, int64_t n, double* out,
+                                               void* stream) {
+    if (n < 0 || (n > 0 && (!vel3 || !mass)) || !out) return fail(MD_ERR_INVALID, "md_kinetic_energy_noalloc: bad arguments");
+    const int64_t nb = (n + kChunk - 1) / kChunk;
+    if (nb > kNoAllocMaxBlocks)
+        return fail(MD_ERR_INVALID, "md_kinetic_energy_noalloc: n = " + std::to_string(n) + " exceeds the maximum of " +
+                                        std::to_string(kNoAllocMaxBlocks * kChunk) + " particles");
+    int device = 0;
+    MD_CUDA(cudaGetDevice(&device));
+    double2* scratch = nullptr;
+    MD_TRY(noalloc_scratch(device, &scratch));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    g_launches = nullptr;
+    double* result = reinterpret_cast<double*>(scratch + kNoAllocMaxBlocks);
+    // Every block partial that the sum reads is written first by k_kinetic_blocks, and the result slot is
+    // written whole by k_sum_blocks, so nothing left by an earlier call is read and nothing needs clearing.
+    if (nb > 0) {
+        const size_t smem = kEnergyWarps * kChunk * sizeof(double);
+        k_kinetic_blocks<<<blocks_for(nb, kEnergyWarps), kEnergyWarps * 32, smem, st>>>(
+            vel3, mass, static_cast<int>(n), scratch, static_cast<int>(nb));
+        MD_CHECK_LAUNCH();
+    }
+    // (sum of the .x partials, sum of the .y partials) into the result slot; .x is the kinetic energy
+    k_sum_blocks<<<1, 32, 0, st>>>(scratch, static_cast<int>(nb), result);
+    MD_CHECK_LAUNCH();
+    MD_CUDA(cudaMemcpyAsync(out, result, sizeof(double), cudaMemcpyDeviceToDevice, st));
+    return MD_OK;
+}
