@@ -54,6 +54,9 @@ def args_parse():
     p.add_argument("--fp64-steps", type=int, default=100, help="steps of the FP64 comparison run (0: skip)")
     p.add_argument("--cpu-steps", type=int, default=3, help="reference steps in the cpu_baseline sample (0: skip)")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--sweep", choices=["precision"], default=None,
+                   help="instead of the headline line: the N=256,000 precision sweep over densities {0.5, 0.8442, 1.0} "
+                        "x T {0.71, 1.5, 3.0} (one JSON line per state point; --steps NVE steps each)")
     p.add_argument("--profile-region", action="store_true",
                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return p.parse_args()
@@ -185,6 +188,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ---- ranks -------------------------------------------------------------------------------------------------
+
+def max_over_ranks(x: float) -> float:
+    """Max of a per-rank time over all ranks of the default process group (NCCL on GPUs, gloo on CPUs)."""
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, n_atoms: int, steps: int, max_ms: float) -> float:
+    """Whole-job atom-steps/s of `world` independent replicas, timed by the slowest rank."""
+    return world * n_atoms * steps / (max_ms / 1e3)
+
+
 # ---- GPU arm ------------------------------------------------------------------------------------------------
 
 def measured_peak():
@@ -292,9 +313,7 @@ def run_gpu_arm(a):
     rebuilds = nl.rebuild_count - rb0
     pairs = nl.pair_count
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms)
         dist.barrier()
     e0 = pe[0] + ke[0]
     drift = float(np.abs((pe + ke - e0) / e0).max())
@@ -357,12 +376,10 @@ def run_gpu_arm(a):
         x1.synchronize()
         ems = x0.elapsed_time(x1)
         if dist:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+            ems = max_over_ranks(ems)
         h2d = n * (32 + 24 + 8)
         d2h = n * (32 + 24) + a.steps * 3 * 8
-        e2e = {"value": world * n * a.steps / (ems / 1e3), "unit": "atom-steps/s",
+        e2e = {"value": replica_throughput(world, n, a.steps, ems), "unit": "atom-steps/s",
                "h2d_bytes_per_step": h2d / a.steps, "d2h_bytes_per_step": d2h / a.steps,
                "includes": "pinned H2D of positions/velocities/masses, list build, initial forces, all steps with "
                            "per-step PE/KE/virial read back, D2H of final positions/velocities"}
@@ -382,7 +399,7 @@ def run_gpu_arm(a):
     bytes_per_atom = 16 + 24 + 4 * 2 * pairs / n  # own float4, fixed-point force, full-list int32 indices
     achieved = bytes_per_atom * n / kernel_s / 1e9
     tpa = ncu_traffic_per_atom()
-    value = world * n * a.steps / (ms / 1e3)
+    value = replica_throughput(world, n, a.steps, ms)
     line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": {"fp32fx": "f32+i64", "fp32": "f32", "fp64": "f64"}[a.precision],
@@ -400,10 +417,66 @@ def run_gpu_arm(a):
         dist.destroy_process_group()
 
 
+# ---- precision sweep (the N = 256,000 density x temperature grid) -------------------------------------------
+
+def precision_sweep(cells=40, densities=(0.5, 0.8442, 1.0), temperatures=(0.71, 1.5, 3.0), steps=10000,
+                    equil=200, rdf_every=100, device=0):
+    """For each state point: melt/rescale equilibration (T = 2 for the first third, then T, every 10 steps),
+    force errors of the float modes against FP64 on the equilibrated state, then `steps` NVE steps from that
+    same state in each precision. Yields one dict per state point: per-particle force errors, energy drift
+    (max |E - E0| / |E0| and its per-step slope), mean virial pressure P = (2K + W) / 3V, the largest g(r)
+    difference from the FP64 run (g(r) from the run's list pairs to r_c every `rdf_every` steps) and
+    atom-steps/s."""
+    import numpy as np
+
+    import mdgpu as md
+
+    for rho in densities:
+        for temp in temperatures:
+            s = md.fcc_system(cells, rho, temp, seed=42, device=device)
+            nl = md.NeighbourList(2.5, 0.3)
+            ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=md.PREC_FP64)
+            integ = md.VelocityVerletIntegrator(0.005)
+            nl.build(s)
+            ff.compute_forces(s, nl)
+            integ.run(s, ff, nl, equil, thermostat="rescale", rescale_every=10, rescale_temperature=temp,
+                      melt_until=equil // 3, melt_temperature=2.0, record=False)
+            errors = force_errors(md, s, nl)
+            start = s.download()
+            vol = s.box ** 3
+            runs = {}
+            for name, prec in (("fp64", md.PREC_FP64), ("fp32fx", md.PREC_FP32FX), ("fp32", md.PREC_FP32)):
+                r = md.System.from_arrays(start["pos"], s.box, vel=start["vel"], force=start["force"], device=device)
+                rl = md.NeighbourList(2.5, 0.3)
+                rf = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)
+                rl.build(r)
+                pe0 = rf.compute_forces(r, rl)
+                e0 = r.kinetic_energy() + pe0
+                rdf = md.RadialDistribution(2.5, 100)
+                t0 = time.perf_counter()
+                pe, ke, w = integ.run(r, rf, rl, steps, rdf=rdf, rdf_every=rdf_every)
+                dt = time.perf_counter() - t0
+                e = pe + ke
+                dev = np.abs((e - e0) / e0)
+                slope = float(np.polyfit(np.arange(1, steps + 1), (e - e0) / abs(e0), 1)[0])
+                runs[name] = {"max_drift": float(dev.max()), "drift_per_step": slope,
+                              "pressure": float(np.mean((2.0 * ke + w) / (3.0 * vol))),
+                              "g": rdf.values(), "atom_steps_per_s": r.n * steps / dt, "rebuilds": rl.rebuild_count}
+            out = {"density": rho, "temperature": temp, "n_atoms": s.n, "steps": steps, "force_error_vs_fp64": errors}
+            g_ref = runs["fp64"]["g"]
+            for name, rr in runs.items():
+                rr["max_dg_vs_fp64"] = float(np.abs(rr.pop("g") - g_ref).max())
+                out[name] = rr
+            yield out
+
+
 def main():
     a = args_parse()
     if a.impl == "reference":
         run_reference_arm(a)
+    elif a.sweep == "precision":
+        for line in precision_sweep(steps=a.steps):
+            print(json.dumps(line), flush=True)
     else:
         run_gpu_arm(a)
 

@@ -137,6 +137,17 @@ md_status md_nlist_update(md_nlist* nl, md_system* s, int* rebuilt);
 /* getPairCount, getRebuildCount, the cell grid side of the last build, hasReverseIndex. Any may be NULL. */
 md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_count, int* cells_per_side,
                         int* reverse_index);
+/* Force kernel choice for one precision: -1 autotunes (the first force call of the list times the global-gather
+ * and the shared-memory tile kernels and keeps the faster), 0 pins global gathers, 1 pins the tile kernel
+ * (used only while the list has tiles). Every variant gives the same bits. md_nlist_force_variant reports the
+ * variant in use (-1 until the first force call). */
+md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant);
+md_status md_nlist_force_variant(const md_nlist* nl, int precision, int* variant);
+/* Layout of the last build (diagnostics): whether the shared-memory tile kernels are in use, the segment
+ * length in cells, segments per cell column, the largest staged tile (particles) and the row capacity.
+ * Any pointer may be NULL. */
+md_status md_nlist_layout(const md_nlist* nl, int* use_tiles, int* segment_cells, int* segments_per_column,
+                          int* max_staged, int* row_capacity);
 /* The half list in the reference's CSR form: offsets[n + 1] (firstPairOf), neighbours[pairs]
  * (neighboursOf in candidate order) and, when the list has a reverse index, rev_offsets[n + 1] and
  * rev_pairs[pairs] (pairsAsSecond). Any may be NULL. */

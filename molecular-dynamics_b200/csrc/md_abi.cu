@@ -8,6 +8,7 @@
 #include "md_fp64.cuh"
 #include "md_nlist.cuh"
 #include "md_scan.cuh"
+#include "md_tiles.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -80,6 +81,9 @@ inline unsigned blocks_for(long long n, int threads) {
 }
 
 constexpr int kThreads = 256;
+// Dynamic shared memory above this gets the opt-in attribute: static shared memory (at most 16 KB in these
+// kernels) counts against the same 48 KB default, so the threshold leaves room for it.
+constexpr size_t kSmemNoOptIn = 32 * 1024;
 
 // Slots of md_system::scal (device scalars)
 constexpr int kScalFactor = 1;  // [1] velocity scale factor, [2] 1 to apply it / 0 to skip
@@ -114,6 +118,7 @@ struct md_system {
 struct CellGrid {
     int ncps = 0, ncells = 0;
     DevBuf<int> cell_of, count, start, cursor;
+    DevBuf<int> max_occ;  // largest cell occupancy of the last sort
     DevBuf<uint32_t> bucket, order;
     DevBuf<long long> tiles;
 };
@@ -141,6 +146,10 @@ struct md_nlist {
     DevBuf<long long> half_off, rev_off, tiles;
     DevBuf<double4> ref_pos;
     DevBuf<float4> frames;  // per-particle float coordinates for the float kernels (n + 1, sentinel last)
+    bool use_tiles = false; // shared-memory tile kernels (3+ cells per side and tiles that fit)
+    TileGeom tiles_geom{};
+    int variant[3] = {-1, -1, -1};  // force kernel per precision (0 global gathers, 1 tile; -1 untuned)
+    int pinned[3] = {-1, -1, -1};   // set by md_nlist_set_force_variant
     int rebuilds = 0;
     uint64_t pairs = 0;
     bool built = false;
@@ -236,6 +245,8 @@ md_status cell_sort(CellGrid& g, md_system* s, double min_size) {
     MD_CUDA(g.tiles.reserve(scan_tiles_needed(g.ncells)));
     MD_CUDA(cudaMemsetAsync(g.count.p, 0, sizeof(int) * g.ncells, s->stream));
     MD_CUDA(cudaMemsetAsync(g.cursor.p, 0, sizeof(int) * g.ncells, s->stream));
+    MD_CUDA(g.max_occ.reserve(1));
+    MD_CUDA(cudaMemsetAsync(g.max_occ.p, 0, sizeof(int), s->stream));
     if (n > 0) {
         k_cell_assign<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(s->pos.p, n, inv_cell, g.ncps, g.cell_of.p,
                                                                            g.count.p);
@@ -248,7 +259,7 @@ md_status cell_sort(CellGrid& g, md_system* s, double min_size) {
                                                                             g.bucket.p);
         MD_CHECK_LAUNCH();
         k_cell_rank<<<blocks_for(static_cast<long long>(g.ncells) * 32, kThreads), kThreads, 0, s->stream>>>(
-            g.start.p, g.ncells, g.bucket.p, g.order.p);
+            g.start.p, g.ncells, g.bucket.p, g.order.p, g.max_occ.p);
         MD_CHECK_LAUNCH();
     }
     return MD_OK;
@@ -262,6 +273,46 @@ int initial_capacity(const md_nlist* nl, const md_system* s) {
     int cap = static_cast<int>(1.35 * est) + 24;
     return (cap + 7) & ~7;
 }
+
+// Defined in md_abi_float.inl
+md_status frames_async(md_system* s, md_nlist* nl);
+CellOffsets cell_offsets(const md_nlist* nl, const md_system* s);
+
+// Segment length and shared-memory size of the tile kernels for this build. Segments aim at ~96 home
+// particles per block. The largest staged tile of the geometry is measured on the device (the cells only
+// change at rebuilds, so it holds until the next one); it must fit 3072 slots (96 KB of double4 for the
+// FP64 kernel), shrinking kk down to one cell. Beyond 6000 slots the global-gather kernels are used instead.
+md_status tile_geometry(md_nlist* nl, md_system* s, bool* use) {
+    *use = false;
+    const int nc = nl->grid.ncps;
+    if (nc < 3 || s->n == 0) return MD_OK;
+    const double avg = static_cast<double>(s->n) / (static_cast<double>(nc) * nc * nc);
+    int kk = static_cast<int>(std::lround(96.0 / std::max(avg, 1.0)));
+    kk = std::clamp(kk, 1, std::min(kMaxSegment, nc - 2));
+    TileGeom& g = nl->tiles_geom;
+    for (;;) {
+        g.ncps = nc;
+        g.kk = kk;
+        g.nseg = (nc + kk - 1) / kk;
+        g.cell = s->box.L / nc;
+        g.box = s->box;
+        MD_CUDA(cudaMemsetAsync(nl->flags.p + 2, 0, sizeof(int), s->stream));
+        const long long segs = static_cast<long long>(nc) * nc * g.nseg;
+        k_tile_max_staged<<<blocks_for(segs, 128), 128, 0, s->stream>>>(nl->grid.start.p, g, nl->flags.p + 2);
+        MD_CHECK_LAUNCH();
+        int staged = 0;
+        MD_CUDA(cudaMemcpyAsync(&staged, nl->flags.p + 2, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        MD_TRY(sync(s));
+        g.max_staged = std::max(staged, 1);
+        if (staged <= 3072 || kk == 1) {
+            *use = staged <= 6000;
+            return MD_OK;
+        }
+        --kk;
+    }
+}
+
+unsigned tile_blocks(const TileGeom& g) { return static_cast<unsigned>(g.ncps) * g.ncps * g.nseg; }
 
 // NeighbourList::build (src/NeighbourList.cpp:55-134) on the device. The reference builds the cell list,
 // reorders the system, and builds the cell list again; the second build only recomputes the cells of the
@@ -290,17 +341,39 @@ md_status nlist_build(md_nlist* nl, md_system* s) {
     }
     s->layout++;
     nl->use_cells = nl->grid.ncps >= 3;  // src/NeighbourList.cpp:69
-    if (nl->cap == 0 || nl->n != s->n) nl->cap = initial_capacity(nl, s);
+    if (nl->cap == 0 || nl->n != s->n) {
+        nl->cap = initial_capacity(nl, s);
+        for (int& v : nl->variant) v = -1;  // a new system: tune the force kernels again
+    }
     MD_CUDA(nl->counts.reserve(n));
     MD_CUDA(nl->flags.reserve(4));
     MD_CUDA(nl->half_off.reserve(n + 1));
     MD_CUDA(nl->tmp_counts.reserve(n));
     MD_CUDA(nl->tiles.reserve(scan_tiles_needed(n)));
+    nl->use_tiles = false;
+    if (nl->use_cells && n > 0) {
+        MD_TRY(frames_async(s, nl));  // float frames of the new cells (the tile build's prefilter reads them)
+        MD_TRY(tile_geometry(nl, s, &nl->use_tiles));
+    }
+    const uint32_t sentinel = static_cast<uint32_t>(n) | (kSentinelCode << kCodeShift);
     for (int attempt = 0; attempt < 4; ++attempt) {
-        MD_CUDA(nl->rows.reserve(static_cast<size_t>(n) * nl->cap));
+        MD_CUDA(nl->rows.reserve(row_buffer_entries(n, nl->cap)));
         MD_CUDA(cudaMemsetAsync(nl->flags.p, 0, 4 * sizeof(int), s->stream));
-        ListGeom geo{s->box, nl->rl2, nl->grid.ncps, nl->use_cells ? 1 : 0, nl->cap, static_cast<uint32_t>(n)};
-        if (n > 0) {
+        if (n > 0 && nl->use_tiles) {
+            const TileGeom& tg = nl->tiles_geom;
+            const double margin = 1e-5 * nl->rl2 + 1e-4;  // float r^2 error is below 1e-5 here
+            BuildParams bp{nl->rl2, static_cast<float>(nl->rl2 - margin), static_cast<float>(nl->rl2 + margin),
+                           nl->cap, static_cast<uint32_t>(n)};
+            const size_t smem = sizeof(float4) * tg.max_staged;
+            if (smem > kSmemNoOptIn)
+                MD_CUDA(cudaFuncSetAttribute(k_nlist_build_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem)));
+            k_nlist_build_tile<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
+                nl->frames.p, s->pos.p, nl->grid.start.p, nl->cell_sorted.p, tg, bp, cell_offsets(nl, s), nl->rows.p,
+                nl->counts.p, nl->flags.p + 1);
+            MD_CHECK_LAUNCH();
+        } else if (n > 0) {
+            ListGeom geo{s->box, nl->rl2, nl->grid.ncps, nl->use_cells ? 1 : 0, nl->cap, sentinel};
             k_nlist_build<<<blocks_for(n, 128), 128, 0, s->stream>>>(s->pos.p, n, geo, nl->cell_sorted.p,
                                                                       nl->grid.start.p, nl->rows.p, nl->counts.p,
                                                                       nl->flags.p + 1);
@@ -336,7 +409,8 @@ bool nlist_current(const md_nlist* nl, const md_system* s) {
 }
 
 // Defined in md_abi_float.inl and below
-md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy);
+md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt,
+                                  bool frames_fresh, bool* fused_ke);
 md_status rdf_sample_async(md_rdf* r, md_system* s, md_nlist* nl);
 md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
                     const md_run_options& o, double* pe, double* ke, double* virial);
@@ -370,18 +444,87 @@ md_status profile_collect(md_system* s) {
     return MD_OK;
 }
 
-// List forces into s->force; energies (pe, virial, inside) into ff->out on the device when want_energy
-md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy) {
+// Autotuner of the list force kernel: with tiles available, the first force call of a list (per precision)
+// times the global-gather kernel (variant 0) and the shared-memory tile kernel (variant 1) on the current
+// state, two launches each after a warm-up, and keeps the faster. Both variants give the same bits, so the
+// choice never changes a result. md_nlist_set_force_variant pins a variant instead.
+template <typename Launch>
+md_status choose_variant(md_system* s, md_nlist* nl, int prec, Launch&& launch) {
+    if (!nl->use_tiles) {
+        nl->variant[prec] = 0;
+        return MD_OK;
+    }
+    if (nl->variant[prec] >= 0) return MD_OK;
+    if (nl->pinned[prec] >= 0) {
+        nl->variant[prec] = nl->pinned[prec];
+        return MD_OK;
+    }
+    cudaEvent_t e0, e1;
+    MD_CUDA(cudaEventCreate(&e0));
+    MD_CUDA(cudaEventCreate(&e1));
+    float best = 0.f;
+    int pick = 0;
+    for (int v = 0; v < 2; ++v) {
+        MD_TRY(launch(v));
+        MD_CUDA(cudaEventRecord(e0, s->stream));
+        MD_TRY(launch(v));
+        MD_TRY(launch(v));
+        MD_CUDA(cudaEventRecord(e1, s->stream));
+        MD_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        MD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (v == 0 || ms < best) {
+            best = ms;
+            pick = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    nl->variant[prec] = pick;
+    return MD_OK;
+}
+
+// A step's force stage. What it leaves behind:
+//   - list forces in s->force;
+//   - with want_energy, (pe, virial) in ff->out and the inside-cutoff count in ff->inside_count;
+//   - with kick_dt > 0, the closing half kick (VelocityVerletIntegrator::kick) applied to the velocities.
+// frames_fresh tells the float kernels that the frames already match the positions (the fused drift wrote
+// them). Returns through *fused_ke whether the fused kick also left the step's kinetic energy in
+// s->scal[kScalKE] (float tile kernels only; fixed-point, not the reference's summation order).
+md_status kick_async(md_system* s, double dt);
+md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt = 0.0,
+                            bool frames_fresh = false, bool* fused_ke = nullptr) {
     const int n = static_cast<int>(s->n);
+    if (fused_ke) *fused_ke = false;
     MD_CUDA(ff->out.reserve(4));
     MD_CUDA(ff->inside_count.reserve(1));
     MD_CUDA(cudaMemsetAsync(ff->inside_count.p, 0, sizeof(unsigned long long), s->stream));
     if (ff->precision == MD_PREC_FP64) {
         if (n > 0) {
+            // variant 0: global gathers; variant 1: shared-memory tile (both bit-identical)
+            auto launch = [&](int variant, bool kick) -> md_status {
+                if (variant == 1) {
+                    const TileGeom& tg = nl->tiles_geom;
+                    const size_t smem = sizeof(double4) * tg.max_staged;
+                    if (smem > kSmemNoOptIn)
+                        MD_CUDA(cudaFuncSetAttribute(k_force_fp64_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     static_cast<int>(smem)));
+                    const KickArgs ka{kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
+                    k_force_fp64_tile<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
+                        s->pos.p, n, nl->grid.start.p, nl->cell_sorted.p, tg, ff->lj, nl->rows.p, nl->cap,
+                        nl->counts.p, s->force.p, ff->inside_count.p, ka);
+                } else {
+                    k_force_fp64<<<blocks_for(n, 128), 128, 0, s->stream>>>(
+                        s->pos.p, n, s->box, ff->lj, nl->rows.p, nl->cap, nl->counts.p, s->force.p, ff->inside_count.p,
+                        kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt);
+                }
+                MD_CHECK_LAUNCH();
+                return MD_OK;
+            };
+            MD_TRY(choose_variant(s, nl, MD_PREC_FP64, [&](int v) { return launch(v, false); }));
+            MD_CUDA(cudaMemsetAsync(ff->inside_count.p, 0, sizeof(unsigned long long), s->stream));
             MD_TRY(profile_mark(s));
-            k_force_fp64<<<blocks_for(n, 128), 128, 0, s->stream>>>(s->pos.p, n, s->box, ff->lj, nl->rows.p, nl->cap,
-                                                                     nl->counts.p, s->force.p, ff->inside_count.p);
-            MD_CHECK_LAUNCH();
+            MD_TRY(launch(nl->variant[MD_PREC_FP64], kick_dt > 0.0));
             MD_TRY(profile_mark(s));
         }
         if (want_energy) {
@@ -402,7 +545,7 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
             }
         }
     } else {
-        MD_TRY(forces_list_float_async(ff, s, nl, want_energy));
+        MD_TRY(forces_list_float_async(ff, s, nl, want_energy, kick_dt, frames_fresh, fused_ke));
     }
     return MD_OK;
 }
@@ -421,14 +564,42 @@ md_status read_energy(md_forcefield* ff, md_system* s, double* pe, double* viria
     return MD_OK;
 }
 
-md_status kick_drift_async(md_system* s, md_nlist* nl, double dt, bool check_skin) {
+// Half kick + drift + wrap; with check_skin also the list's half-skin test into nl->flags[0]; with
+// write_frames also the float frames of the new positions (the list must be current and use tiles).
+md_status kick_drift_async(md_system* s, md_nlist* nl, double dt, bool check_skin, bool write_frames = false) {
     const int n = static_cast<int>(s->n);
     if (n == 0) return MD_OK;
     if (check_skin) MD_CUDA(cudaMemsetAsync(nl->flags.p, 0, sizeof(int), s->stream));
-    k_kick_drift<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(
-        s->pos.p, s->vel.p, s->force.p, s->mass.p, n, 0.5 * dt, dt, s->box, check_skin ? nl->ref_pos.p : nullptr,
-        nl ? nl->max_disp2 : 0.0, check_skin ? nl->flags.p : nullptr);
+    if (write_frames) {
+        const TileGeom& tg = nl->tiles_geom;
+        k_kick_drift_frames<<<blocks_for(n + 1, kThreads), kThreads, 0, s->stream>>>(
+            s->pos.p, s->vel.p, s->force.p, s->mass.p, n, 0.5 * dt, dt, s->box, check_skin ? nl->ref_pos.p : nullptr,
+            nl->max_disp2, check_skin ? nl->flags.p : nullptr, nl->cell_sorted.p, tg.ncps, tg.cell, nl->frames.p);
+    } else {
+        k_kick_drift<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(
+            s->pos.p, s->vel.p, s->force.p, s->mass.p, n, 0.5 * dt, dt, s->box, check_skin ? nl->ref_pos.p : nullptr,
+            nl ? nl->max_disp2 : 0.0, check_skin ? nl->flags.p : nullptr);
+    }
     MD_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+// The first half of VelocityVerletIntegrator::step (src/Integrator.cpp:18-30): kick, drift and wrap, then
+// NeighbourList::update. The staleness flag is read back (one 4-byte copy); a stale or never-built list is
+// rebuilt. Afterwards the float frames match the positions whenever the list uses tiles.
+md_status drift_and_update(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, bool* rebuilt) {
+    const bool current = nlist_current(nl, s);
+    const bool frames = current && nl->use_tiles && ff->precision != MD_PREC_FP64;
+    MD_TRY(kick_drift_async(s, nl, dt, current, frames));
+    bool stale = true;
+    if (current) {
+        int flag = 0;
+        MD_CUDA(cudaMemcpyAsync(&flag, nl->flags.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        MD_TRY(sync(s));
+        stale = flag != 0;
+    }
+    if (stale) MD_TRY(nlist_build(nl, s));
+    *rebuilt = stale;
     return MD_OK;
 }
 
@@ -860,6 +1031,32 @@ md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_c
     return MD_OK;
 }
 
+md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant) {
+    if (!nl || precision < MD_PREC_FP64 || precision > MD_PREC_FP32 || variant < -1 || variant > 1)
+        return fail(MD_ERR_INVALID, "md_nlist_set_force_variant: bad arguments");
+    nl->pinned[precision] = variant;
+    nl->variant[precision] = -1;
+    return MD_OK;
+}
+
+md_status md_nlist_force_variant(const md_nlist* nl, int precision, int* variant) {
+    if (!nl || !variant || precision < MD_PREC_FP64 || precision > MD_PREC_FP32)
+        return fail(MD_ERR_INVALID, "md_nlist_force_variant: bad arguments");
+    *variant = nl->variant[precision];
+    return MD_OK;
+}
+
+md_status md_nlist_layout(const md_nlist* nl, int* use_tiles, int* segment_cells, int* segments_per_column,
+                          int* max_staged, int* row_capacity) {
+    if (!nl) return fail(MD_ERR_INVALID, "null list");
+    if (use_tiles) *use_tiles = nl->use_tiles ? 1 : 0;
+    if (segment_cells) *segment_cells = nl->tiles_geom.kk;
+    if (segments_per_column) *segments_per_column = nl->tiles_geom.nseg;
+    if (max_staged) *max_staged = nl->tiles_geom.max_staged;
+    if (row_capacity) *row_capacity = nl->cap;
+    return MD_OK;
+}
+
 md_status md_nlist_download(md_nlist* nl, uint64_t* offsets, uint64_t* neighbours, uint64_t* rev_offsets,
                             uint64_t* rev_pairs) {
     if (!nl) return fail(MD_ERR_INVALID, "null list");
@@ -1000,20 +1197,10 @@ md_status md_step_list(md_system* s, md_forcefield* ff, md_nlist* nl, double dt,
     if (ff->deterministic && !nl->reverse)
         return fail(MD_ERR_NO_REVERSE_INDEX, "Deterministic forces need a NeighbourList built with reverseIndex = true");
     ff->device = s->device;
-    const bool current = nlist_current(nl, s);
-    MD_TRY(kick_drift_async(s, nl, dt, current));
     bool stale = true;
-    if (current) {
-        int flag = 0;
-        MD_CUDA(cudaMemcpyAsync(&flag, nl->flags.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-        MD_TRY(sync(s));
-        stale = flag != 0;
-        if (!stale) nl->layout = s->layout;
-    }
-    if (stale) MD_TRY(nlist_build(nl, s));
+    MD_TRY(drift_and_update(s, ff, nl, dt, &stale));
     if (rebuilt) *rebuilt = stale ? 1 : 0;
-    MD_TRY(forces_list_async(ff, s, nl, true));
-    MD_TRY(kick_async(s, dt));
+    MD_TRY(forces_list_async(ff, s, nl, true, dt, true));
     return read_energy(ff, s, pe, nullptr, nullptr);
 }
 

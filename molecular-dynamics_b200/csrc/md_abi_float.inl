@@ -11,6 +11,10 @@ FloatLJ float_lj(const md_forcefield* ff) {
     f.eps4 = static_cast<float>(ff->lj.eps4);
     f.shift = static_cast<float>(ff->lj.shift);
     f.rc2 = static_cast<float>(ff->lj.rc2);
+    // the float r^2 of a pair is within ~1e-5 of the exact value (frames are cell-relative), so this shell
+    // holds every pair whose float and double cutoff tests could disagree
+    f.band = static_cast<float>(1e-5 * ff->lj.rc2 + 1e-4);
+    f.rc2d = ff->lj.rc2;
     return f;
 }
 
@@ -38,43 +42,96 @@ md_status frames_async(md_system* s, md_nlist* nl) {
     return MD_OK;
 }
 
-md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy) {
+// See forces_list_async. Every float kernel fuses the closing kick with a fixed-point kinetic energy.
+md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt,
+                                  bool frames_fresh, bool* fused_ke) {
     const int n = static_cast<int>(s->n);
     const bool fixed = ff->precision == MD_PREC_FP32FX;
+    const bool kick = kick_dt > 0.0;
     const FloatLJ lj = float_lj(ff);
     MD_CUDA(ff->fx_acc.reserve(4));
-    if (want_energy) MD_CUDA(cudaMemsetAsync(ff->fx_acc.p, 0, 3 * sizeof(long long), s->stream));
+    if (want_energy || kick) MD_CUDA(cudaMemsetAsync(ff->fx_acc.p, 0, 4 * sizeof(long long), s->stream));
     auto* acc = reinterpret_cast<unsigned long long*>(ff->fx_acc.p);
     if (n > 0) {
         const unsigned g = blocks_for(n, 128);
-        if (nl->use_cells) MD_TRY(frames_async(s, nl));
-        const CellOffsets offs = nl->use_cells ? cell_offsets(nl, s) : CellOffsets{};
-        // one launch of the float force kernel matching (cells, fixed point, energy)
-        auto launch = [&](auto fixed_tag, auto energy_tag) {
-            constexpr bool kF = decltype(fixed_tag)::value;
-            constexpr bool kE = decltype(energy_tag)::value;
-            if (nl->use_cells)
-                k_force_fp32<kF, kE><<<g, 128, 0, s->stream>>>(nl->frames.p, n, lj, offs, nl->rows.p, nl->cap,
-                                                               nl->counts.p, s->force.p, acc);
-            else
-                k_force_fp32_small<kF, kE><<<g, 128, 0, s->stream>>>(s->pos.p, n, s->box, lj, nl->rows.p, nl->cap,
-                                                                     nl->counts.p, s->force.p, acc);
-        };
-        using T = std::true_type;
-        using F = std::false_type;
-        MD_TRY(profile_mark(s));
-        if (fixed) {
-            if (want_energy) launch(T{}, T{}); else launch(T{}, F{});
+        if (nl->use_cells) {
+            // variant 0: global gathers (k_force_fp32_rows); variant 1: shared-memory tile (same bits)
+            if (!frames_fresh) MD_TRY(frames_async(s, nl));
+            const TileGeom& tg = nl->tiles_geom;
+            const CellOffsets offs = cell_offsets(nl, s);
+            const size_t smem = sizeof(float4) * (tg.max_staged + 1);
+            auto launch = [&](int variant, bool with_kick, bool energy) -> md_status {
+                const KickArgs ka{with_kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
+                auto go = [&](auto rows_kernel, auto tile_kernel) -> md_status {
+                    if (variant == 1) {
+                        if (smem > kSmemNoOptIn)
+                            MD_CUDA(cudaFuncSetAttribute(tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                         static_cast<int>(smem)));
+                        tile_kernel<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
+                            nl->frames.p, s->pos.p, n, nl->grid.start.p, nl->cell_sorted.p, tg, lj, offs, nl->rows.p,
+                            nl->cap, nl->counts.p, s->force.p, acc, ka);
+                    } else {
+                        rows_kernel<<<g, 128, 0, s->stream>>>(nl->frames.p, s->pos.p, n, s->box, lj, offs, nl->rows.p,
+                                                              nl->cap, nl->counts.p, s->force.p, acc, ka);
+                    }
+                    MD_CHECK_LAUNCH();
+                    return MD_OK;
+                };
+                if (fixed)
+                    return energy ? go(k_force_fp32_rows<true, true>, k_force_fp32_tile<true, true>)
+                                  : go(k_force_fp32_rows<true, false>, k_force_fp32_tile<true, false>);
+                return energy ? go(k_force_fp32_rows<false, true>, k_force_fp32_tile<false, true>)
+                              : go(k_force_fp32_rows<false, false>, k_force_fp32_tile<false, false>);
+            };
+            MD_TRY(choose_variant(s, nl, ff->precision, [&](int v) { return launch(v, false, false); }));
+            if (want_energy || kick) MD_CUDA(cudaMemsetAsync(ff->fx_acc.p, 0, 4 * sizeof(long long), s->stream));
+            MD_TRY(profile_mark(s));
+            MD_TRY(launch(nl->variant[ff->precision], kick, want_energy));
+            MD_TRY(profile_mark(s));
         } else {
-            if (want_energy) launch(F{}, T{}); else launch(F{}, F{});
+            const KickArgs ka{kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
+            MD_TRY(profile_mark(s));
+            if (fixed) {
+                if (want_energy)
+                    k_force_fp32_small<true, true><<<g, 128, 0, s->stream>>>(s->pos.p, n, s->box, lj, nl->rows.p,
+                                                                             nl->cap, nl->counts.p, s->force.p, acc, ka);
+                else
+                    k_force_fp32_small<true, false><<<g, 128, 0, s->stream>>>(s->pos.p, n, s->box, lj, nl->rows.p,
+                                                                              nl->cap, nl->counts.p, s->force.p, acc, ka);
+            } else {
+                if (want_energy)
+                    k_force_fp32_small<false, true><<<g, 128, 0, s->stream>>>(s->pos.p, n, s->box, lj, nl->rows.p,
+                                                                              nl->cap, nl->counts.p, s->force.p, acc, ka);
+                else
+                    k_force_fp32_small<false, false><<<g, 128, 0, s->stream>>>(s->pos.p, n, s->box, lj, nl->rows.p,
+                                                                               nl->cap, nl->counts.p, s->force.p, acc, ka);
+            }
+            MD_CHECK_LAUNCH();
+            MD_TRY(profile_mark(s));
         }
-        MD_CHECK_LAUNCH();
-        MD_TRY(profile_mark(s));
     }
-    if (want_energy) {
-        k_finish_float_energy<<<1, 1, 0, s->stream>>>(acc, ff->out.p, ff->inside_count.p);
+    const bool ke_fused = kick && n > 0;
+    if (want_energy || ke_fused) {
+        k_finish_float_energy<<<1, 1, 0, s->stream>>>(acc, ff->out.p, ff->inside_count.p,
+                                                      ke_fused ? s->scal.p + kScalKE : nullptr, 1.0 / kKineticScale);
         MD_CHECK_LAUNCH();
     }
+    if (fused_ke) *fused_ke = ke_fused;
+    return MD_OK;
+}
+
+// Fixed-point kinetic energy of the current velocities into s->scal[kScalKE] (float runs)
+md_status kinetic_fixed_async(md_system* s, md_forcefield* ff) {
+    const int n = static_cast<int>(s->n);
+    MD_CUDA(ff->fx_acc.reserve(4));
+    auto* acc = reinterpret_cast<unsigned long long*>(ff->fx_acc.p) + 3;
+    MD_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long), s->stream));
+    if (n > 0) {
+        k_kinetic_fixed<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(s->vel.p, s->mass.p, n, acc);
+        MD_CHECK_LAUNCH();
+    }
+    k_fixed_to_double<<<1, 1, 0, s->stream>>>(acc, 1.0 / kKineticScale, s->scal.p + kScalKE);
+    MD_CHECK_LAUNCH();
     return MD_OK;
 }
 
@@ -88,7 +145,7 @@ md_status rdf_sample_async(md_rdf* r, md_system* s, md_nlist* nl) {
     const int n = static_cast<int>(s->n);
     if (n > 0) {
         const size_t smem = sizeof(unsigned int) * r->bins;
-        if (smem > 48 * 1024)
+        if (smem > kSmemNoOptIn)
             MD_CUDA(cudaFuncSetAttribute(k_rdf_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         k_rdf_sample<<<blocks_for(n, kThreads), kThreads, smem, s->stream>>>(
             s->pos.p, n, s->box, nl->rows.p, nl->cap, nl->counts.p, r->rmax * r->rmax, r->bin_width, r->bins, r->hist.p);
@@ -102,8 +159,10 @@ md_status rdf_sample_async(md_rdf* r, md_system* s, md_nlist* nl) {
     return MD_OK;
 }
 
-// md_run's step loop. This version drives the step from the host and reads the half-skin flag after each
-// drift (one 4-byte copy per step), then rebuilds on the host's decision.
+// md_run's step loop. The step is driven from the host, which reads the half-skin flag after each drift (one
+// 4-byte copy per step) and rebuilds on its decision. Kinetic energies: FP64 runs use the reference's blocked
+// summation order (so thermostats stay bit-identical); float runs use the fixed-point kinetic energy the force
+// kernel fuses with the closing kick, and recompute it after a thermostat.
 md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
                     const md_run_options& o, double* pe, double* ke, double* virial) {
     const double bussi_c = o.thermostat == 2 ? std::exp(-dt / o.bussi_tau) : 0.0;  // src/Thermostat.cpp:46
@@ -117,40 +176,33 @@ md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, in
     DevBuf<double> rec;  // per step: pe, virial, ke
     if (n_steps > 0) MD_CUDA(rec.reserve(3 * static_cast<size_t>(n_steps)));
     const bool want_energy = pe || virial;
+    const bool exact_ke = ff->precision == MD_PREC_FP64;
     for (int64_t k = 0; k < n_steps; ++k) {
         const int64_t step = o.first_step + k;
-        const bool current = nlist_current(nl, s);
-        MD_TRY(kick_drift_async(s, nl, dt, current));
-        bool stale = true;
-        if (current) {
-            int flag = 0;
-            MD_CUDA(cudaMemcpyAsync(&flag, nl->flags.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-            MD_TRY(sync(s));
-            stale = flag != 0;
-            if (!stale) nl->layout = s->layout;
-        }
-        if (stale) MD_TRY(nlist_build(nl, s));
-        MD_TRY(forces_list_async(ff, s, nl, want_energy));
-        MD_TRY(kick_async(s, dt));
-        if (want_energy) {
+        bool rebuilt = false, fused_ke = false;
+        MD_TRY(drift_and_update(s, ff, nl, dt, &rebuilt));
+        MD_TRY(forces_list_async(ff, s, nl, want_energy, dt, true, &fused_ke));
+        if (want_energy)
             MD_CUDA(cudaMemcpyAsync(rec.p + 3 * k, ff->out.p, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
-        }
-        if (o.thermostat == 1 && o.rescale_every > 0 && step % o.rescale_every == 0) {
-            const double target = step <= o.melt_until ? o.melt_temperature : o.rescale_temperature;
-            MD_TRY(kinetic_async(s));
-            k_rescale_factor<<<1, 1, 0, s->stream>>>(s->scal.p + kScalKE, dof_of(s->n), target, s->scal.p + kScalFactor);
+        bool ke_current = fused_ke && !exact_ke;  // scal[kScalKE] holds this step's kinetic energy
+        const bool rescale = o.thermostat == 1 && o.rescale_every > 0 && step % o.rescale_every == 0;
+        if (rescale || o.thermostat == 2) {
+            if (!ke_current) MD_TRY(kinetic_async(s));
+            if (rescale) {
+                const double target = step <= o.melt_until ? o.melt_temperature : o.rescale_temperature;
+                k_rescale_factor<<<1, 1, 0, s->stream>>>(s->scal.p + kScalKE, dof_of(s->n), target,
+                                                         s->scal.p + kScalFactor);
+            } else {
+                k_bussi_factor<<<1, 1, 0, s->stream>>>(s->scal.p + kScalKE, dof_of(s->n), o.bussi_temperature, bussi_c,
+                                                       noise.p + k, noise.p + n_steps + k, s->scal.p + kScalFactor);
+            }
             MD_CHECK_LAUNCH();
             MD_TRY(scale_async(s));
-        } else if (o.thermostat == 2) {
-            MD_TRY(kinetic_async(s));
-            k_bussi_factor<<<1, 1, 0, s->stream>>>(s->scal.p + kScalKE, dof_of(s->n), o.bussi_temperature, bussi_c,
-                                                   noise.p + k, noise.p + n_steps + k, s->scal.p + kScalFactor);
-            MD_CHECK_LAUNCH();
-            MD_TRY(scale_async(s));
+            ke_current = false;
         }
         if (o.rdf && o.rdf_every > 0 && step % o.rdf_every == 0) MD_TRY(rdf_sample_async(o.rdf, s, nl));
         if (ke) {
-            MD_TRY(kinetic_async(s));
+            if (!ke_current) MD_TRY(exact_ke ? kinetic_async(s) : kinetic_fixed_async(s, ff));
             MD_CUDA(cudaMemcpyAsync(rec.p + 3 * k + 2, s->scal.p + kScalKE, sizeof(double), cudaMemcpyDeviceToDevice,
                                     s->stream));
         }

@@ -42,13 +42,15 @@ __global__ void k_cell_scatter(const int* __restrict__ cell_of, int n, const int
 // One warp per cell: each particle's rank in its cell is the number of smaller indices in the bucket, so
 // order[] lists every cell's particles in increasing index, as the reference's serial scatter does
 // (src/CellList.cpp:48-51).
+// max_occ receives the largest cell occupancy (it sizes the shared-memory tiles).
 __global__ void k_cell_rank(const int* __restrict__ start, int ncells, const uint32_t* __restrict__ bucket,
-                            uint32_t* __restrict__ order) {
+                            uint32_t* __restrict__ order, int* __restrict__ max_occ) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= ncells) return;
     const int s = start[warp];
     const int m = start[warp + 1] - s;
+    if (lane == 0) atomicMax(max_occ, m);
     for (int e = lane; e < m; e += 32) {
         const uint32_t v = bucket[s + e];
         int rank = 0;

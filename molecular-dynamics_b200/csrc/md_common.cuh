@@ -14,6 +14,19 @@ constexpr int kCodeShift = 27;                       // neighbour entry: j in bi
 constexpr uint32_t kIndexMask = (1u << kCodeShift) - 1u;
 constexpr int kMaxParticles = (1 << kCodeShift) - 2; // one slot is the sentinel
 constexpr int kChunk = 1024;                         // deterministicSum block (include/Parallel.hpp:34)
+constexpr uint32_t kSentinelCode = 31u;              // cell code of row padding entries (j = n, the sentinel)
+
+// Neighbour rows are "uint4-interleaved" per group of 32 consecutive particles: entries [4q, 4q + 4) of
+// particle i form the uint4 at index ((i >> 5) * cap / 4 + q) * 32 + (i & 31), so a warp of consecutive
+// particles reading one uint4 each touches 512 contiguous bytes. cap is a multiple of 8. The row buffer
+// must hold ceil(n / 32) * 32 * cap entries.
+__host__ __device__ __forceinline__ size_t row_index(int i, int s, int cap) {
+    return ((static_cast<size_t>(i >> 5) * (cap >> 2) + (s >> 2)) * 32 + (i & 31)) * 4 + (s & 3);
+}
+__device__ __forceinline__ uint4 row_quad(const uint32_t* __restrict__ rows, int i, int q, int cap) {
+    return reinterpret_cast<const uint4*>(rows)[(static_cast<size_t>(i >> 5) * (cap >> 2) + q) * 32 + (i & 31)];
+}
+inline size_t row_buffer_entries(long long n, int cap) { return static_cast<size_t>((n + 31) / 32) * 32 * cap; }
 
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }

@@ -1,4 +1,7 @@
-// Float pair arithmetic for the list forces (precision modes MD_PREC_FP32FX and MD_PREC_FP32).
+// Float pair arithmetic for the list forces (precision modes MD_PREC_FP32FX and MD_PREC_FP32): frames, the
+// shared pair/epilogue helpers, the global-gather kernel and the small-box kernel. The shared-memory tile
+// kernel is in md_tiles.cuh; both evaluate every pair with the same pinned float operation sequence
+// (float_pair), so either one gives the same bits.
 //
 // Positions enter the pair loop as float offsets from the centre of each particle's cell at the last list
 // build (a "frame"), refreshed from the double positions every step. A pair's separation is
@@ -22,6 +25,7 @@ constexpr float kForceScale = 4294967296.0f;        // 2^32: fixed-point units p
 constexpr double kForceUnit = 1.0 / 4294967296.0;
 constexpr float kEnergyScale = 16777216.0f;         // 2^24 for energy and virial sums
 constexpr double kEnergyUnit = 1.0 / 16777216.0;
+constexpr double kKineticScale = 4294967296.0;      // 2^32: fixed-point units of the fused kinetic energy
 constexpr float kSentinelCoord = 1.0e15f;           // frame of the sentinel particle: never inside the cutoff
 
 struct FloatLJ {
@@ -31,11 +35,119 @@ struct FloatLJ {
     float eps4;    // 4 eps
     float shift;   // energy shift
     float rc2;     // cut_off^2
+    float band;    // |float r^2 - r_c^2| below this: decide inside/outside with the exact double test
+    double rc2d;   // cut_off^2 in double
 };
 
 struct CellOffsets {
-    float4 off[27];  // -d * cell for the 27 codes (d in {-1, 0, 1}^3)
+    float4 off[32];  // -d * cell for the 27 codes (d in {-1, 0, 1}^3); zero for the sentinel code
 };
+
+// The closing half kick fused into a force kernel (vel == nullptr: forces only)
+struct KickArgs {
+    double* vel;
+    const double* mass;
+    double half_dt;
+};
+
+// The truncated potential's force jumps by |F(r_c)| at the cutoff, so a pair whose float r^2 sits within
+// rounding of r_c^2 must be classified as the reference classifies it: min-image r^2 < r_c^2 in double
+// (src/Forcefield.cpp:366). Only pairs in a thin shell take this branch.
+__device__ __forceinline__ bool exact_inside(const double4& a, const double4& b, const Box& box, double rc2) {
+    const double dx = min_image(dsub(a.x, b.x), box);
+    const double dy = min_image(dsub(a.y, b.y), box);
+    const double dz = min_image(dsub(a.z, b.z), box);
+    return norm2(dx, dy, dz) < rc2;
+}
+
+// One pair in float with a pinned operation sequence (explicit roundings and FMAs), shared by every float
+// kernel. Adds its force to (gx, gy, gz) and, with kEnergy, its energy, virial and inside count.
+template <bool kEnergy>
+__device__ __forceinline__ void float_pair(float dx, float dy, float dz, bool in, float r2, const FloatLJ& lj,
+                                           float& gx, float& gy, float& gz, float& ge, float& gw,
+                                           unsigned long long& ins) {
+    const float inv = __frcp_rn(r2);
+    const float sr2 = __fmul_rn(lj.sig2, inv);
+    const float sr6 = __fmul_rn(__fmul_rn(sr2, sr2), sr2);
+    float fr = __fmul_rn(__fmul_rn(fmaf(lj.eps48, sr6, -lj.eps24), sr6), inv);
+    fr = in ? fr : 0.0f;
+    gx = fmaf(fr, dx, gx);
+    gy = fmaf(fr, dy, gy);
+    gz = fmaf(fr, dz, gz);
+    if (kEnergy) {
+        const float en = fmaf(__fmul_rn(lj.eps4, sr6), __fadd_rn(sr6, -1.0f), -lj.shift);
+        ge = __fadd_rn(ge, in ? en : 0.0f);
+        gw = fmaf(fr, r2, gw);
+        ins += in ? 1u : 0u;
+    }
+}
+
+// Separation of a row entry's pair from the frames: (q_i - q_j) + image offset, and its float r^2
+__device__ __forceinline__ float float_separation(const float4& qi, const float4& qj, const float4& o, float& dx,
+                                                  float& dy, float& dz) {
+    dx = __fadd_rn(__fsub_rn(qi.x, qj.x), o.x);
+    dy = __fadd_rn(__fsub_rn(qi.y, qj.y), o.y);
+    dz = __fadd_rn(__fsub_rn(qi.z, qj.z), o.z);
+    return fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
+}
+
+// Per-particle accumulators of the float kernels: a group of 8 row entries goes into fixed point (FP32FX) or
+// into the running float sum (FP32)
+template <bool kFixed, bool kEnergy>
+struct FloatAcc {
+    long long ax = 0, ay = 0, az = 0;
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+    __device__ __forceinline__ void add_group(float gx, float gy, float gz, float ge, float gw, long long& e_fx,
+                                              long long& w_fx) {
+        if (kFixed) {
+            ax += __float2ll_rn(gx * kForceScale);
+            ay += __float2ll_rn(gy * kForceScale);
+            az += __float2ll_rn(gz * kForceScale);
+        } else {
+            fx = __fadd_rn(fx, gx);
+            fy = __fadd_rn(fy, gy);
+            fz = __fadd_rn(fz, gz);
+        }
+        if (kEnergy) {
+            e_fx += __float2ll_rn(ge * kEnergyScale);
+            w_fx += __float2ll_rn(gw * kEnergyScale);
+        }
+    }
+    // Write the force (double, component-major) and apply the fused closing kick; returns the particle's
+    // fixed-point kinetic energy after the kick (0 without a kick)
+    __device__ __forceinline__ long long finish(int i, int n, double* __restrict__ force, const KickArgs& kick) const {
+        const double F[3] = {kFixed ? static_cast<double>(ax) * kForceUnit : static_cast<double>(fx),
+                             kFixed ? static_cast<double>(ay) * kForceUnit : static_cast<double>(fy),
+                             kFixed ? static_cast<double>(az) * kForceUnit : static_cast<double>(fz)};
+        double ke = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const size_t o = static_cast<size_t>(k) * n + i;
+            force[o] = F[k];
+            if (kick.vel) {  // VelocityVerletIntegrator::kick (src/Integrator.cpp:55-71)
+                const double v = dadd(kick.vel[o], ddiv(dmul(kick.half_dt, F[k]), kick.mass[i]));
+                kick.vel[o] = v;
+                ke = dadd(ke, dmul(v, v));
+            }
+        }
+        return kick.vel ? __double2ll_rn(dmul(dmul(dmul(0.5, kick.mass[i]), ke), kKineticScale)) : 0;
+    }
+};
+
+// Block-level sums of the fixed-point energy, virial, inside count and kinetic energy into acc[0..3]
+__device__ __forceinline__ void flush_sums(long long e_fx, long long w_fx, unsigned long long ins, long long k_fx,
+                                           unsigned long long* __restrict__ acc) {
+    e_fx = warp_sum_i64(e_fx);
+    w_fx = warp_sum_i64(w_fx);
+    k_fx = warp_sum_i64(k_fx);
+    ins = warp_sum_u64(ins);
+    if ((threadIdx.x & 31) == 0) {
+        if (e_fx) atomicAdd(&acc[0], static_cast<unsigned long long>(e_fx));
+        if (w_fx) atomicAdd(&acc[1], static_cast<unsigned long long>(w_fx));
+        if (ins) atomicAdd(&acc[2], ins);
+        if (k_fx) atomicAdd(&acc[3], static_cast<unsigned long long>(k_fx));
+    }
+}
 
 // Frames: q = minimum-image (r - centre of the particle's build cell), in float. frames[n] is the sentinel.
 __global__ void k_frames(const double4* __restrict__ pos, int n, const int* __restrict__ cell_sorted, int ncps,
@@ -53,176 +165,92 @@ __global__ void k_frames(const double4* __restrict__ pos, int n, const int* __re
     frames[i] = make_float4(static_cast<float>(dx), static_cast<float>(dy), static_cast<float>(dz), 0.0f);
 }
 
-// One thread per particle over its full row (own and reverse partners, padded with sentinels to a multiple
-// of 8). kFixed selects FP32FX; kEnergy adds the energy, virial and inside-pair sums (every pair is seen
-// twice, from both ends, so the host halves them).
+// Thread per particle over its row with neighbour frames gathered from global memory (L1/L2); rows are read
+// as interleaved uint4, coalesced across the warp.
 template <bool kFixed, bool kEnergy>
-__global__ void __launch_bounds__(128) k_force_fp32(const float4* __restrict__ frames, int n, FloatLJ lj,
-                                                     CellOffsets offs, const uint32_t* __restrict__ rows, int cap,
-                                                     const int2* __restrict__ counts, double* __restrict__ force,
-                                                     unsigned long long* __restrict__ acc) {
-    __shared__ float4 s_off[27];
-    if (threadIdx.x < 27) s_off[threadIdx.x] = offs.off[threadIdx.x];
+__global__ void __launch_bounds__(128) k_force_fp32_rows(const float4* __restrict__ frames,
+                                                         const double4* __restrict__ pos, int n, Box box,
+                                                         FloatLJ lj, CellOffsets offs,
+                                                         const uint32_t* __restrict__ rows, int cap,
+                                                         const int2* __restrict__ counts, double* __restrict__ force,
+                                                         unsigned long long* __restrict__ acc, KickArgs kick) {
+    __shared__ float4 s_off[32];
+    if (threadIdx.x < 32) s_off[threadIdx.x] = offs.off[threadIdx.x];
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    long long e_fx = 0, w_fx = 0;
+    long long e_fx = 0, w_fx = 0, k_fx = 0;
     unsigned long long ins = 0;
     if (i < n) {
         const float4 qi = frames[i];
-        const uint4* row = reinterpret_cast<const uint4*>(rows + static_cast<size_t>(i) * cap);
         const int2 c = counts[i];
-        const int groups = (c.x + c.y + 7) >> 3;
-        long long ax = 0, ay = 0, az = 0;
-        float fx = 0.f, fy = 0.f, fz = 0.f;
+        const int groups = (c.x + c.y + 7) >> 3;  // rows are padded with sentinels to a multiple of 8
+        FloatAcc<kFixed, kEnergy> a;
         for (int g = 0; g < groups; ++g) {
-            const uint4 e0 = row[2 * g], e1 = row[2 * g + 1];
+            const uint4 e0 = row_quad(rows, i, 2 * g, cap);
+            const uint4 e1 = row_quad(rows, i, 2 * g + 1, cap);
             const uint32_t ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
             float gx = 0.f, gy = 0.f, gz = 0.f, ge = 0.f, gw = 0.f;
 #pragma unroll
-            for (int t = 0; t < 8; ++t) {
-                const uint32_t e = ent[t];
-                const float4 qj = frames[e & kIndexMask];
-                const float4 o = s_off[e >> kCodeShift];
-                const float dx = (qi.x - qj.x) + o.x;
-                const float dy = (qi.y - qj.y) + o.y;
-                const float dz = (qi.z - qj.z) + o.z;
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const bool in = r2 < lj.rc2;
-                const float inv = __frcp_rn(r2);
-                const float sr2 = lj.sig2 * inv;
-                const float sr6 = sr2 * sr2 * sr2;
-                float fr = (lj.eps48 * sr6 - lj.eps24) * sr6 * inv;
-                fr = in ? fr : 0.0f;
-                gx = fmaf(fr, dx, gx);
-                gy = fmaf(fr, dy, gy);
-                gz = fmaf(fr, dz, gz);
-                if (kEnergy) {
-                    const float en = fmaf(lj.eps4 * sr6, sr6 - 1.0f, -lj.shift);
-                    ge += in ? en : 0.0f;
-                    gw = fmaf(fr, r2, gw);
-                    ins += in ? 1u : 0u;
-                }
+            for (int u = 0; u < 8; ++u) {
+                const uint32_t e = ent[u];
+                const int j = static_cast<int>(e & kIndexMask);
+                float dx, dy, dz;
+                const float r2 = float_separation(qi, frames[j], s_off[e >> kCodeShift], dx, dy, dz);
+                bool in = r2 < lj.rc2;
+                if (fabsf(r2 - lj.rc2) < lj.band) in = exact_inside(pos[i], pos[j], box, lj.rc2d);
+                float_pair<kEnergy>(dx, dy, dz, in, r2, lj, gx, gy, gz, ge, gw, ins);
             }
-            if (kFixed) {
-                ax += __float2ll_rn(gx * kForceScale);
-                ay += __float2ll_rn(gy * kForceScale);
-                az += __float2ll_rn(gz * kForceScale);
-            } else {
-                fx += gx;
-                fy += gy;
-                fz += gz;
-            }
-            if (kEnergy) {
-                e_fx += __float2ll_rn(ge * kEnergyScale);
-                w_fx += __float2ll_rn(gw * kEnergyScale);
-            }
+            a.add_group(gx, gy, gz, ge, gw, e_fx, w_fx);
         }
-        double Fx, Fy, Fz;
-        if (kFixed) {
-            Fx = static_cast<double>(ax) * kForceUnit;
-            Fy = static_cast<double>(ay) * kForceUnit;
-            Fz = static_cast<double>(az) * kForceUnit;
-        } else {
-            Fx = fx;
-            Fy = fy;
-            Fz = fz;
-        }
-        force[i] = Fx;
-        force[static_cast<size_t>(n) + i] = Fy;
-        force[2 * static_cast<size_t>(n) + i] = Fz;
+        k_fx = a.finish(i, n, force, kick);
     }
-    if (kEnergy) {
-        e_fx = warp_sum_i64(e_fx);
-        w_fx = warp_sum_i64(w_fx);
-        ins = warp_sum_u64(ins);
-        if ((threadIdx.x & 31) == 0) {
-            atomicAdd(&acc[0], static_cast<unsigned long long>(e_fx));
-            atomicAdd(&acc[1], static_cast<unsigned long long>(w_fx));
-            atomicAdd(&acc[2], ins);
-        }
-    }
+    if (kEnergy || kick.vel) flush_sums(e_fx, w_fx, ins, k_fx, acc);
 }
 
 // Boxes under 3 cells per side (all-pairs candidates): separations come from the double positions with the
 // reference's minimum image, then narrow to float (the reference's mixed path does the same,
-// src/Forcefield.cpp:373-386).
+// src/Forcefield.cpp:373-386); the cutoff test uses the double r^2.
 template <bool kFixed, bool kEnergy>
 __global__ void k_force_fp32_small(const double4* __restrict__ pos, int n, Box box, FloatLJ lj,
                                    const uint32_t* __restrict__ rows, int cap, const int2* __restrict__ counts,
-                                   double* __restrict__ force, unsigned long long* __restrict__ acc) {
+                                   double* __restrict__ force, unsigned long long* __restrict__ acc, KickArgs kick) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    long long e_fx = 0, w_fx = 0;
+    long long e_fx = 0, w_fx = 0, k_fx = 0;
     unsigned long long ins = 0;
     if (i < n) {
         const double4 pi = pos[i];
-        const uint32_t* row = rows + static_cast<size_t>(i) * cap;
         const int2 c = counts[i];
         const int m = c.x + c.y;
-        long long ax = 0, ay = 0, az = 0;
-        float fx = 0.f, fy = 0.f, fz = 0.f;
+        FloatAcc<kFixed, kEnergy> a;
         for (int g0 = 0; g0 < m; g0 += 8) {
             float gx = 0.f, gy = 0.f, gz = 0.f, ge = 0.f, gw = 0.f;
             for (int s = g0; s < g0 + 8 && s < m; ++s) {
-                const double4 pj = pos[row[s] & kIndexMask];
-                double ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
-                ddx -= box.L * round(ddx * box.invL);
-                ddy -= box.L * round(ddy * box.invL);
-                ddz -= box.L * round(ddz * box.invL);
+                const double4 pj = pos[rows[row_index(i, s, cap)] & kIndexMask];
+                const double ddx = min_image(dsub(pi.x, pj.x), box);
+                const double ddy = min_image(dsub(pi.y, pj.y), box);
+                const double ddz = min_image(dsub(pi.z, pj.z), box);
                 const float dx = static_cast<float>(ddx), dy = static_cast<float>(ddy), dz = static_cast<float>(ddz);
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const bool in = r2 < lj.rc2;
-                const float inv = __frcp_rn(r2);
-                const float sr2 = lj.sig2 * inv;
-                const float sr6 = sr2 * sr2 * sr2;
-                float fr = (lj.eps48 * sr6 - lj.eps24) * sr6 * inv;
-                fr = in ? fr : 0.0f;
-                gx = fmaf(fr, dx, gx);
-                gy = fmaf(fr, dy, gy);
-                gz = fmaf(fr, dz, gz);
-                if (kEnergy) {
-                    const float en = fmaf(lj.eps4 * sr6, sr6 - 1.0f, -lj.shift);
-                    ge += in ? en : 0.0f;
-                    gw = fmaf(fr, r2, gw);
-                    ins += in ? 1u : 0u;
-                }
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
+                const bool in = norm2(ddx, ddy, ddz) < lj.rc2d;  // the reference's cutoff test, in double
+                float_pair<kEnergy>(dx, dy, dz, in, r2, lj, gx, gy, gz, ge, gw, ins);
             }
-            if (kFixed) {
-                ax += __float2ll_rn(gx * kForceScale);
-                ay += __float2ll_rn(gy * kForceScale);
-                az += __float2ll_rn(gz * kForceScale);
-            } else {
-                fx += gx;
-                fy += gy;
-                fz += gz;
-            }
-            if (kEnergy) {
-                e_fx += __float2ll_rn(ge * kEnergyScale);
-                w_fx += __float2ll_rn(gw * kEnergyScale);
-            }
+            a.add_group(gx, gy, gz, ge, gw, e_fx, w_fx);
         }
-        force[i] = kFixed ? static_cast<double>(ax) * kForceUnit : static_cast<double>(fx);
-        force[static_cast<size_t>(n) + i] = kFixed ? static_cast<double>(ay) * kForceUnit : static_cast<double>(fy);
-        force[2 * static_cast<size_t>(n) + i] = kFixed ? static_cast<double>(az) * kForceUnit : static_cast<double>(fz);
+        k_fx = a.finish(i, n, force, kick);
     }
-    if (kEnergy) {
-        e_fx = warp_sum_i64(e_fx);
-        w_fx = warp_sum_i64(w_fx);
-        ins = warp_sum_u64(ins);
-        if ((threadIdx.x & 31) == 0) {
-            atomicAdd(&acc[0], static_cast<unsigned long long>(e_fx));
-            atomicAdd(&acc[1], static_cast<unsigned long long>(w_fx));
-            atomicAdd(&acc[2], ins);
-        }
-    }
+    if (kEnergy || kick.vel) flush_sums(e_fx, w_fx, ins, k_fx, acc);
 }
 
-// Converts the fixed-point energy sums to (pe, virial) doubles, halving the double-counted pairs; the
-// inside count goes to *inside as an integer.
+// Converts the fixed-point sums to doubles: (pe, virial) with the double-counted pairs halved into out[0..1],
+// the inside count (halved, an integer) into *inside, and, when ke_out is set, the fused kinetic energy
+// (2^-32 units) into *ke_out.
 __global__ void k_finish_float_energy(const unsigned long long* __restrict__ acc, double* __restrict__ out,
-                                      unsigned long long* __restrict__ inside) {
+                                      unsigned long long* __restrict__ inside, double* __restrict__ ke_out,
+                                      double kinetic_unit) {
     out[0] = 0.5 * static_cast<double>(static_cast<long long>(acc[0])) * kEnergyUnit;
     out[1] = 0.5 * static_cast<double>(static_cast<long long>(acc[1])) * kEnergyUnit;
     *inside = acc[2] / 2;
+    if (ke_out) *ke_out = static_cast<double>(static_cast<long long>(acc[3])) * kinetic_unit;
 }
 
 }  // namespace md

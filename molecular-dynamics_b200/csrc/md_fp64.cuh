@@ -13,18 +13,19 @@ namespace md {
 // its own pairs in list order, then subtracts F(j, i) over the pairs where it is second, in increasing pair
 // index. Pairs outside the cutoff contribute an exact zero in the reference and are skipped here. The
 // inside-cutoff count is the number of own pairs with r^2 < r_c^2 (a sum of whole numbers, exact).
+// With kick_vel set it also applies the closing half kick, v += (half_dt F) / m, with k_kick's sequence.
 __global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ lj, const uint32_t* __restrict__ rows,
                              int cap, const int2* __restrict__ counts, double* __restrict__ force,
-                             unsigned long long* __restrict__ inside) {
+                             unsigned long long* __restrict__ inside, double* __restrict__ kick_vel,
+                             const double* __restrict__ mass, double half_dt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long ins = 0;
     if (i < n) {
         const double4 pi = pos[i];
-        const uint32_t* row = rows + static_cast<size_t>(i) * cap;
         const int2 c = counts[i];
         double fx = 0.0, fy = 0.0, fz = 0.0;
         for (int s = 0; s < c.x; ++s) {
-            const double4 pj = pos[row[s] & kIndexMask];
+            const double4 pj = pos[rows[row_index(i, s, cap)] & kIndexMask];
             const double dx = min_image(dsub(pi.x, pj.x), box);
             const double dy = min_image(dsub(pi.y, pj.y), box);
             const double dz = min_image(dsub(pi.z, pj.z), box);
@@ -38,7 +39,7 @@ __global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ
             ++ins;
         }
         for (int s = c.x; s < c.x + c.y; ++s) {
-            const double4 pj = pos[row[s] & kIndexMask];
+            const double4 pj = pos[rows[row_index(i, s, cap)] & kIndexMask];
             const double dx = min_image(dsub(pj.x, pi.x), box);
             const double dy = min_image(dsub(pj.y, pi.y), box);
             const double dz = min_image(dsub(pj.z, pi.z), box);
@@ -50,9 +51,13 @@ __global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ
             fy = dsub(fy, dmul(f, dy));
             fz = dsub(fz, dmul(f, dz));
         }
-        force[i] = fx;
-        force[static_cast<size_t>(n) + i] = fy;
-        force[2 * static_cast<size_t>(n) + i] = fz;
+        const double F[3] = {fx, fy, fz};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const size_t o = static_cast<size_t>(k) * n + i;
+            force[o] = F[k];
+            if (kick_vel) kick_vel[o] = dadd(kick_vel[o], ddiv(dmul(half_dt, F[k]), mass[i]));
+        }
     }
     ins = warp_sum_u64(ins);
     if ((threadIdx.x & 31) == 0 && ins) atomicAdd(inside, ins);
@@ -90,9 +95,8 @@ __global__ void k_energy_blocks_fp64(const double4* __restrict__ pos, int n, Box
         const long long kb = b > k0 ? b : k0;
         const long long ke = half_off[i + 1] < k1 ? half_off[i + 1] : k1;
         const double4 pi = pos[i];
-        const uint32_t* row = rows + static_cast<size_t>(i) * cap;
         for (long long k = kb + lane; k < ke; k += 32) {
-            const double4 pj = pos[row[k - b] & kIndexMask];
+            const double4 pj = pos[rows[row_index(i, static_cast<int>(k - b), cap)] & kIndexMask];
             const double dx = min_image(dsub(pi.x, pj.x), box);
             const double dy = min_image(dsub(pi.y, pj.y), box);
             const double dz = min_image(dsub(pi.z, pj.z), box);
@@ -277,10 +281,9 @@ __global__ void k_rdf_sample(const double4* __restrict__ pos, int n, Box box, co
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         const double4 pi = pos[i];
-        const uint32_t* row = rows + static_cast<size_t>(i) * cap;
         const int own = counts[i].x;
         for (int s = 0; s < own; ++s) {
-            const double4 pj = pos[row[s] & kIndexMask];
+            const double4 pj = pos[rows[row_index(i, s, cap)] & kIndexMask];
             const double dx = min_image(dsub(pi.x, pj.x), box);
             const double dy = min_image(dsub(pi.y, pj.y), box);
             const double dz = min_image(dsub(pi.z, pj.z), box);

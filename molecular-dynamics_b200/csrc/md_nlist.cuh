@@ -1,13 +1,13 @@
 // Verlet neighbour list build on the cell-sorted system (src/NeighbourList.cpp:55-134).
 //
-// Device layout: one fixed-capacity row of `cap` 32-bit entries per particle (row i at rows[i * cap]).
-// Row i holds, in order:
+// Device layout: one fixed-capacity row of `cap` 32-bit entries per particle, stored uint4-interleaved
+// (row_index in md_common.cuh). Row i holds, in order:
 //   1. its own pairs j > i in the reference's candidate order (27 cells in (dx, dy, dz) order,
 //      src/CellList.cpp:55-83, then increasing j inside each cell, src/NeighbourList.cpp:38-52) — exactly
 //      neighboursOf(i);
 //   2. the particles j < i that list i as a neighbour, in increasing j — the pairs pairsAsSecond(i) of the
 //      reference's reverse index, in the same order (a pair's global index grows with its first particle);
-//   3. sentinel entries up to a multiple of 8.
+//   3. sentinel entries (n | kSentinelCode << 27) up to a multiple of 8.
 // Each entry is j | (cell code << 27), the code being (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1) of the
 // neighbour cell, used by the float kernels to rebuild the periodic image. A pair is in the list when its
 // minimum-image r^2 < (r_c + skin)^2 in the reference's double arithmetic; the test is symmetric in (i, j)
@@ -54,10 +54,9 @@ __global__ void k_nlist_build(const double4* __restrict__ pos, int n, ListGeom g
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double4 pi = pos[i];
-    uint32_t* row = rows + static_cast<size_t>(i) * g.cap;
     int cnt = 0;
     auto push = [&](int j, uint32_t code) {
-        if (cnt < g.cap) row[cnt] = static_cast<uint32_t>(j) | (code << kCodeShift);
+        if (cnt < g.cap) rows[row_index(i, cnt, g.cap)] = static_cast<uint32_t>(j) | (code << kCodeShift);
         ++cnt;
     };
     int own;
@@ -107,7 +106,7 @@ __global__ void k_nlist_build(const double4* __restrict__ pos, int n, ListGeom g
     }
     counts[i] = make_int2(own, cnt - own);
     const int padded = (cnt + 7) & ~7;
-    for (int s = cnt; s < padded && s < g.cap; ++s) row[s] = g.sentinel;
+    for (int s = cnt; s < padded && s < g.cap; ++s) rows[row_index(i, s, g.cap)] = g.sentinel;
     atomicMax(max_count, padded);
 }
 
@@ -126,9 +125,8 @@ __global__ void k_half_csr(const uint32_t* __restrict__ rows, int n, int cap, co
                            const long long* __restrict__ half_off, uint64_t* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t* row = rows + static_cast<size_t>(i) * cap;
     const long long b = half_off[i];
-    for (int s = 0; s < counts[i].x; ++s) out[b + s] = row[s] & kIndexMask;
+    for (int s = 0; s < counts[i].x; ++s) out[b + s] = rows[row_index(i, s, cap)] & kIndexMask;
 }
 
 // Reverse CSR for download (pairsAsSecond): the r-th partner j < i of i is the pair whose global index is
@@ -138,15 +136,13 @@ __global__ void k_reverse_pairs(const uint32_t* __restrict__ rows, int n, int ca
                                 uint64_t* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t* row = rows + static_cast<size_t>(i) * cap;
     const int2 c = counts[i];
     const long long b = rev_off[i];
     for (int r = 0; r < c.y; ++r) {
-        const uint32_t j = row[c.x + r] & kIndexMask;
-        const uint32_t* rj = rows + static_cast<size_t>(j) * cap;
+        const int j = static_cast<int>(rows[row_index(i, c.x + r, cap)] & kIndexMask);
         const int own_j = counts[j].x;
         int pos = 0;
-        while (pos < own_j && (rj[pos] & kIndexMask) != static_cast<uint32_t>(i)) ++pos;
+        while (pos < own_j && (rows[row_index(j, pos, cap)] & kIndexMask) != static_cast<uint32_t>(i)) ++pos;
         out[b + r] = static_cast<uint64_t>(half_off[j] + pos);
     }
 }

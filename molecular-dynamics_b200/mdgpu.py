@@ -58,6 +58,8 @@ def _load():
         "md_nlist_create": (_I, [_D, _D, _I, _PP]), "md_nlist_destroy": (_I, [_P]),
         "md_nlist_build": (_I, [_P, _P]), "md_nlist_update": (_I, [_P, _P, _PI]),
         "md_nlist_info": (_I, [_P, _PU64, _PI, _PI, _PI]),
+        "md_nlist_layout": (_I, [_P, _PI, _PI, _PI, _PI, _PI]),
+        "md_nlist_set_force_variant": (_I, [_P, _I, _I]), "md_nlist_force_variant": (_I, [_P, _I, _PI]),
         "md_nlist_download": (_I, [_P, _PU64, _PU64, _PU64, _PU64]),
         "md_forcefield_create": (_I, [_D, _D, _D, _PP]), "md_forcefield_destroy": (_I, [_P]),
         "md_forcefield_shift": (_I, [_P, _PD]), "md_forcefield_set_precision": (_I, [_P, _I]),
@@ -330,6 +332,22 @@ class NeighbourList:
     @property
     def cells_per_side(self) -> int:
         return self._info()[2]
+
+    def set_force_variant(self, precision: int, variant: int):
+        """-1 autotunes the list force kernel; 0 pins global gathers; 1 pins the shared-memory tile kernel."""
+        _check(LIB.md_nlist_set_force_variant(self.h, precision, variant))
+
+    def force_variant(self, precision: int) -> int:
+        v = C.c_int()
+        _check(LIB.md_nlist_force_variant(self.h, precision, C.byref(v)))
+        return v.value
+
+    def layout(self) -> dict:
+        """Tile geometry and row capacity of the last build (diagnostics)."""
+        v = [C.c_int() for _ in range(5)]
+        _check(LIB.md_nlist_layout(self.h, *[C.byref(x) for x in v]))
+        return dict(zip(("use_tiles", "segment_cells", "segments_per_column", "max_staged", "row_capacity"),
+                        (x.value for x in v)))
 
     def download(self):
         P, _, _, rev = self._info()
