@@ -171,6 +171,9 @@ md_status md_forces_list(md_forcefield* ff, md_system* s, md_nlist* nl, double* 
                          double* inside);
 /* computeForces(System&), the O(N^2) path (src/Forcefield.cpp:39-78). */
 md_status md_forces_all_pairs(md_forcefield* ff, md_system* s, double* pe, double* virial, double* inside);
+/* getVirial / getInsidePairs (include/Forcefield.hpp:26-29): the virial and inside-cutoff pair count of the
+ * force field's last evaluation, whether by md_forces_*, md_step_* or md_run. Outputs may be NULL. */
+md_status md_forcefield_results(const md_forcefield* ff, double* virial, double* inside);
 
 /* ---- VelocityVerletIntegrator: include/Integrator.hpp:9-19, src/Integrator.cpp --------------------- */
 /* step(System&, const LennardJonesForceField&, NeighbourList&) (src/Integrator.cpp:18-30): half kick, drift
@@ -209,6 +212,63 @@ md_status md_rdf_sample(md_rdf* r, md_system* s, md_nlist* nl);
 md_status md_rdf_values(md_rdf* r, double* radii, double* g, int* samples);
 /* The raw histogram of pair counts (bins long). */
 md_status md_rdf_histogram(md_rdf* r, double* hist);
+
+/* ---- batched replicas ----------------------------------------------------------------------------------
+ * Many independent systems of uneven size, density and temperature advanced together: each replica follows
+ * the reference's single-system step on its own box (System + NeighbourList(r_c, skin, true) +
+ * LennardJonesForceField with setDeterministic(true) in FP64 + VelocityVerletIntegrator::step + the thermostat,
+ * src/Integrator.cpp:18-30, src/Thermostat.cpp:17-58), with the same bits as that replica run alone through
+ * md_system/md_nlist/md_run. The reference has no batched interface; this one replaces a loop over systems.
+ * Rebuilds are decided per replica on the device, and a run executes as CUDA graphs of chunk_steps steps. */
+typedef struct md_batch md_batch;
+
+typedef struct md_batch_options {
+    double epsilon, sigma, cutoff, skin, dt; /* shared by all replicas */
+    int precision;        /* md_precision */
+    int thermostat;       /* 0 none (NVE), 1 rescaleVelocities to each replica's temperature every rescale_every
+                             steps of a run, 2 Bussi with bussi_tau, drawing per replica like md_bussi_noise */
+    int rescale_every;
+    double bussi_tau;
+    int energy_every;     /* record potential energy, virial and kinetic energy (after the thermostat) of every
+                             replica at every energy_every-th step of a run; 0 records nothing */
+    int chunk_steps;      /* steps per CUDA graph (0: 100), rounded up to a multiple of the thermostat and
+                             sampling periods */
+    int initial_capacity; /* neighbour row capacity (0: estimated from the densest replica); grown on demand */
+} md_batch_options;
+
+/* replicas systems; replica r has n_atoms[r] particles in a box of side box_length[r], target temperature
+ * temperature[r] (thermostats only) and Bussi seed seeds[r] (thermostat 2 only). pos4, vel3 and mass are the
+ * replicas' reference arrays concatenated in replica order: 4 n (x, y, z, pad) positions, 3 n component-major
+ * velocities per replica ([vx(n), vy(n), vz(n)]), n masses (NULL: 1). ids start as 0 .. n-1 per replica.
+ * The list is built and the starting forces computed from it. */
+md_status md_batch_create(int device, int replicas, const int64_t* n_atoms, const double* box_length,
+                          const double* temperature, const uint64_t* seeds, const double* pos4, const double* vel3,
+                          const double* mass, const md_batch_options* opts, md_batch** out);
+md_status md_batch_destroy(md_batch* b);
+/* Replicas, particles (sum of n), neighbour row capacity, kernels launched so far. Any may be NULL. */
+md_status md_batch_info(const md_batch* b, int* replicas, int64_t* atoms, int* capacity, uint64_t* launches);
+md_status md_batch_stream(md_batch* b, void** stream);
+/* n_steps steps of every replica. With energy_every = k, row s of the records (replica r at [s * replicas + r])
+ * is step (s + 1) k of this run; arrays hold n_steps / k rows each and may be NULL. */
+md_status md_batch_run(md_batch* b, int64_t n_steps, double* pe, double* virial, double* ke);
+/* Potential energy, virial, inside-cutoff pair count and kinetic energy of each replica's current state
+ * (replicas entries each; any may be NULL). */
+md_status md_batch_energy(md_batch* b, double* pe, double* virial, double* ke, double* inside);
+/* One replica's arrays in the reference's layout (as md_system_download). Any output may be NULL. */
+md_status md_batch_download(md_batch* b, int replica, double* pos4, double* vel3, double* force3, double* mass,
+                            uint64_t* ids);
+/* System::stateHash of every replica (src/System.cpp:85-105) into hashes[replicas]. */
+md_status md_batch_state_hash(md_batch* b, uint64_t* hashes);
+/* NeighbourList::getRebuildCount of every replica (the first build included) into rebuilds[replicas]. */
+md_status md_batch_rebuilds(md_batch* b, uint64_t* rebuilds);
+/* Force kernel shape: variant -1 autotunes (times every shape and keeps the fastest; done at creation), else
+ * pins one. md_batch_force_variant reports the variant in use, how many there are, and its particles per block
+ * and threads per particle. Every variant gives the same bits. */
+md_status md_batch_set_force_variant(md_batch* b, int variant);
+md_status md_batch_force_variant(const md_batch* b, int* variant, int* count, int* particles_per_block,
+                                 int* threads_per_particle);
+/* Average device time (ms) of the list force kernel alone over reps launches, CUDA events on the batch stream. */
+md_status md_batch_time_forces(md_batch* b, int reps, double* ms);
 
 #ifdef __cplusplus
 }

@@ -2,6 +2,7 @@
 // their device buffers and one CUDA stream per system; every kernel is in the md_*.cuh headers.
 #include "md_b200.h"
 
+#include "md_batch.cuh"
 #include "md_cells.cuh"
 #include "md_common.cuh"
 #include "md_fp32.cuh"
@@ -226,6 +227,19 @@ md_status scale_async(md_system* s) {
 }
 
 double dof_of(int64_t n) { return 3.0 * static_cast<double>(n) - 3.0; }
+
+// src/Forcefield.cpp:8-15 and the constant factors of pairTerms (:25-36)
+LJ lj_constants(double epsilon, double sigma, double cutoff) {
+    const double sr6 = std::pow(sigma / cutoff, 6);
+    const double sr12 = sr6 * sr6;
+    LJ lj{};
+    lj.shift = 4.0 * epsilon * (sr12 - sr6);
+    lj.sig2 = sigma * sigma;
+    lj.eps24 = 24.0 * epsilon;
+    lj.eps4 = 4.0 * epsilon;
+    lj.rc2 = cutoff * cutoff;
+    return lj;
+}
 
 // Counting sort by cell (src/CellList.cpp:9-52) into g.start / g.order; returns ncps
 md_status cell_sort(CellGrid& g, md_system* s, double min_size) {
@@ -675,6 +689,7 @@ md_status md_system_create(int64_t n, double box_length, int device, md_system**
 
 md_status md_system_destroy(md_system* s) {
     if (!s) return MD_OK;
+    if (g_launches == &s->launches) g_launches = nullptr;
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (cudaEvent_t e : s->events) cudaEventDestroy(e);
@@ -1113,14 +1128,7 @@ md_status md_forcefield_create(double epsilon, double sigma, double cutoff, md_f
     ff->eps = epsilon;
     ff->sigma = sigma;
     ff->rc = cutoff;
-    // src/Forcefield.cpp:8-15 and the constant factors of pairTerms (:25-36)
-    const double sr6 = std::pow(sigma / cutoff, 6);
-    const double sr12 = sr6 * sr6;
-    ff->lj.shift = 4.0 * epsilon * (sr12 - sr6);
-    ff->lj.sig2 = sigma * sigma;
-    ff->lj.eps24 = 24.0 * epsilon;
-    ff->lj.eps4 = 4.0 * epsilon;
-    ff->lj.rc2 = cutoff * cutoff;
+    ff->lj = lj_constants(epsilon, sigma, cutoff);
     *out = ff;
     return MD_OK;
 }
@@ -1160,6 +1168,13 @@ md_status md_forces_list(md_forcefield* ff, md_system* s, md_nlist* nl, double* 
     ff->device = s->device;
     MD_TRY(forces_list_async(ff, s, nl, true));
     return read_energy(ff, s, pe, virial, inside);
+}
+
+md_status md_forcefield_results(const md_forcefield* ff, double* virial, double* inside) {
+    if (!ff) return fail(MD_ERR_INVALID, "null force field");
+    if (virial) *virial = ff->virial;
+    if (inside) *inside = ff->inside;
+    return MD_OK;
 }
 
 md_status md_forces_all_pairs(md_forcefield* ff, md_system* s, double* pe, double* virial, double* inside) {
@@ -1357,3 +1372,5 @@ extern "C" md_status md_kinetic_energy_noalloc(const double* vel3, const double*
     MD_CUDA(cudaMemcpyAsync(out, result, sizeof(double), cudaMemcpyDeviceToDevice, st));
     return MD_OK;
 }
+
+#include "md_batch.inl"

@@ -149,20 +149,34 @@ __device__ __forceinline__ void flush_sums(long long e_fx, long long w_fx, unsig
     }
 }
 
+// The frame of a position: minimum-image (r - centre of cell c), narrowed to float. Every kernel that writes
+// frames calls this, with explicit roundings, so all of them produce the same bits.
+__device__ __forceinline__ float4 frame_of(const double4& p, int c, int ncps, double cell, const Box& box) {
+    const int cx = c / (ncps * ncps), cy = (c / ncps) % ncps, cz = c % ncps;
+    double d[3] = {dsub(p.x, dmul(cx + 0.5, cell)), dsub(p.y, dmul(cy + 0.5, cell)), dsub(p.z, dmul(cz + 0.5, cell))};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d[k] = dsub(d[k], dmul(box.L, rint(dmul(d[k], box.invL))));
+    return make_float4(static_cast<float>(d[0]), static_cast<float>(d[1]), static_cast<float>(d[2]), 0.0f);
+}
+
+// The image offset -d * cell of a neighbour-cell code (d in {-1, 0, 1}^3), zero for codes above 26: the same
+// floats the host writes into CellOffsets (-d * cell in double is exact, so only the narrowing rounds)
+__device__ __forceinline__ float4 code_offset(int code, float cell) {
+    if (code > 26) return make_float4(0.f, 0.f, 0.f, 0.f);
+    const int d[3] = {code / 9 - 1, (code / 3) % 3 - 1, code % 3 - 1};
+    float o[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) o[k] = d[k] == 0 ? 0.0f : (d[k] > 0 ? -cell : cell);
+    return make_float4(o[0], o[1], o[2], 0.0f);
+}
+
 // Frames: q = minimum-image (r - centre of the particle's build cell), in float. frames[n] is the sentinel.
 __global__ void k_frames(const double4* __restrict__ pos, int n, const int* __restrict__ cell_sorted, int ncps,
                          double cell, Box box, float4* __restrict__ frames) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) frames[n] = make_float4(kSentinelCoord, kSentinelCoord, kSentinelCoord, 0.0f);
     if (i >= n) return;
-    const int c = cell_sorted[i];
-    const int cx = c / (ncps * ncps), cy = (c / ncps) % ncps, cz = c % ncps;
-    const double4 p = pos[i];
-    double dx = p.x - (cx + 0.5) * cell, dy = p.y - (cy + 0.5) * cell, dz = p.z - (cz + 0.5) * cell;
-    dx -= box.L * rint(dx * box.invL);
-    dy -= box.L * rint(dy * box.invL);
-    dz -= box.L * rint(dz * box.invL);
-    frames[i] = make_float4(static_cast<float>(dx), static_cast<float>(dy), static_cast<float>(dz), 0.0f);
+    frames[i] = frame_of(pos[i], cell_sorted[i], ncps, cell, box);
 }
 
 // Thread per particle over its row with neighbour frames gathered from global memory (L1/L2); rows are read

@@ -239,7 +239,18 @@ __global__ void k_rescale_factor(const double* __restrict__ ke, double dof, doub
     scale[1] = 1.0;
 }
 
-// BussiThermostat::apply, equation A7 (src/Thermostat.cpp:36-58), with r1 and chi2 given
+// BussiThermostat::apply's velocity scale, equation A7 (src/Thermostat.cpp:40-57), for kinetic > 0
+__device__ __forceinline__ double bussi_scale(double kinetic, double dof, double temperature, double c, double r1,
+                                              double chi2) {
+    const double target = dmul(dmul(0.5, dof), temperature);
+    const double omc = dsub(1.0, c);
+    const double t1 = dmul(omc, dsub(ddiv(dmul(target, dadd(chi2, dmul(r1, r1))), dof), kinetic));
+    const double t2 = dmul(dmul(2.0, r1), __dsqrt_rn(dmul(dmul(dmul(ddiv(target, dof), kinetic), omc), c)));
+    const double nk = dadd(dadd(kinetic, t1), t2);
+    return __dsqrt_rn(ddiv(nk, kinetic));
+}
+
+// BussiThermostat::apply (src/Thermostat.cpp:36-58), with r1 and chi2 given
 __global__ void k_bussi_factor(const double* __restrict__ ke, double dof, double temperature, double c,
                                const double* __restrict__ r1p, const double* __restrict__ chi2p,
                                double* __restrict__ scale) {
@@ -248,13 +259,7 @@ __global__ void k_bussi_factor(const double* __restrict__ ke, double dof, double
         scale[1] = 0.0;
         return;
     }
-    const double r1 = r1p[0], chi2 = chi2p[0];
-    const double target = dmul(dmul(0.5, dof), temperature);
-    const double omc = dsub(1.0, c);
-    const double t1 = dmul(omc, dsub(ddiv(dmul(target, dadd(chi2, dmul(r1, r1))), dof), kinetic));
-    const double t2 = dmul(dmul(2.0, r1), __dsqrt_rn(dmul(dmul(dmul(ddiv(target, dof), kinetic), omc), c)));
-    const double nk = dadd(dadd(kinetic, t1), t2);
-    scale[0] = __dsqrt_rn(ddiv(nk, kinetic));
+    scale[0] = bussi_scale(kinetic, dof, temperature, c, r1p[0], chi2p[0]);
     scale[1] = 1.0;
 }
 

@@ -439,15 +439,7 @@ __global__ void k_kick_drift_frames(double4* __restrict__ pos, double* __restric
         const double dz = min_image(dsub(p.z, r.z), box);
         if (norm2(dx, dy, dz) > max_disp2) *stale = 1;
     }
-    if (frames) {
-        const int c = cell_sorted[i];
-        const int cx = c / (ncps * ncps), cy = (c / ncps) % ncps, cz = c % ncps;
-        double fx = p.x - (cx + 0.5) * cell, fy = p.y - (cy + 0.5) * cell, fz = p.z - (cz + 0.5) * cell;
-        fx -= box.L * rint(fx * box.invL);
-        fy -= box.L * rint(fy * box.invL);
-        fz -= box.L * rint(fz * box.invL);
-        frames[i] = make_float4(static_cast<float>(fx), static_cast<float>(fy), static_cast<float>(fz), 0.0f);
-    }
+    if (frames) frames[i] = frame_of(p, cell_sorted[i], ncps, cell, box);
 }
 
 }  // namespace md

@@ -33,6 +33,8 @@ public:
     void setPrecision(Precision p);
 
     md_forcefield* handle() const { return h_; }
+    // Refresh getVirial / getInsidePairs from the device's last evaluation (after an integrator step)
+    void fetchResults() const;
     void setResults(double virial, double inside) const {
         virial_ = virial;
         insidePairs_ = inside;

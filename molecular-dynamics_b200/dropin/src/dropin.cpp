@@ -336,6 +336,12 @@ void LennardJonesForceField::setPrecision(Precision p) {
     check(md_forcefield_set_precision(h_, static_cast<int>(p)));
 }
 
+void LennardJonesForceField::fetchResults() const {
+    double w = 0.0, ins = 0.0;
+    check(md_forcefield_results(h_, &w, &ins));
+    setResults(w, ins);
+}
+
 double LennardJonesForceField::computeForces(System& system) const {
     double pe = 0.0, w = 0.0, ins = 0.0;
     check(md_forces_all_pairs(h_, system.handle(), &pe, &w, &ins));
@@ -358,6 +364,7 @@ double VelocityVerletIntegrator::step(System& system, const LennardJonesForceFie
     double pe = 0.0;
     check(md_step_all_pairs(system.handle(), forceField.handle(), dt_, &pe));
     system.deviceChanged(System::kPositions | System::kVelocities | System::kForces);
+    forceField.fetchResults();
     return pe;
 }
 
@@ -368,6 +375,7 @@ double VelocityVerletIntegrator::step(System& system, const LennardJonesForceFie
     check(md_step_list(system.handle(), forceField.handle(), neighbourList.handle(), dt_, &pe, &rebuilt));
     system.deviceChanged(rebuilt ? System::kAll : (System::kPositions | System::kVelocities | System::kForces));
     if (rebuilt) neighbourList.listChanged();
+    forceField.fetchResults();
     return pe;
 }
 

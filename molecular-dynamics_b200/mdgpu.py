@@ -39,6 +39,13 @@ class md_run_options(C.Structure):
                 ("rdf_every", C.c_int), ("first_step", C.c_int64)]
 
 
+class md_batch_options(C.Structure):
+    _fields_ = [("epsilon", C.c_double), ("sigma", C.c_double), ("cutoff", C.c_double), ("skin", C.c_double),
+                ("dt", C.c_double), ("precision", C.c_int), ("thermostat", C.c_int), ("rescale_every", C.c_int),
+                ("bussi_tau", C.c_double), ("energy_every", C.c_int), ("chunk_steps", C.c_int),
+                ("initial_capacity", C.c_int)]
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`")
@@ -73,6 +80,16 @@ def _load():
         "md_system_stream": (_I, [_P, _PP]), "md_system_synchronize": (_I, [_P]),
         "md_system_launch_count": (_I, [_P, _PU64]), "md_profile_enable": (_I, [_P, _I]),
         "md_profile_read": (_I, [_P, _PD, C.POINTER(C.c_int64)]),
+        "md_forcefield_results": (_I, [_P, _PD, _PD]),
+        "md_batch_create": (_I, [_I, _I, C.POINTER(C.c_int64), _PD, _PD, _PU64, _PD, _PD, _PD,
+                                 C.POINTER(md_batch_options), _PP]),
+        "md_batch_destroy": (_I, [_P]), "md_batch_info": (_I, [_P, _PI, C.POINTER(C.c_int64), _PI, _PU64]),
+        "md_batch_stream": (_I, [_P, _PP]), "md_batch_run": (_I, [_P, _I64, _PD, _PD, _PD]),
+        "md_batch_energy": (_I, [_P, _PD, _PD, _PD, _PD]),
+        "md_batch_download": (_I, [_P, _I, _PD, _PD, _PD, _PD, _PU64]),
+        "md_batch_state_hash": (_I, [_P, _PU64]), "md_batch_rebuilds": (_I, [_P, _PU64]),
+        "md_batch_set_force_variant": (_I, [_P, _I]), "md_batch_force_variant": (_I, [_P, _PI, _PI, _PI, _PI]),
+        "md_batch_time_forces": (_I, [_P, _I, _PD]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -392,6 +409,12 @@ class LennardJonesForceField:
     def set_deterministic(self, deterministic: bool):
         _check(LIB.md_forcefield_set_deterministic(self.h, int(deterministic)))
 
+    def fetch_results(self):
+        """getVirial / getInsidePairs of the last evaluation, steps included (md_forcefield_results)."""
+        w, ins = C.c_double(), C.c_double()
+        _check(LIB.md_forcefield_results(self.h, C.byref(w), C.byref(ins)))
+        self.virial, self.inside_pairs = w.value, ins.value
+
     def compute_forces(self, system: System, neighbour_list: NeighbourList | None = None) -> float:
         pe, w, ins = C.c_double(), C.c_double(), C.c_double()
         if neighbour_list is None:
@@ -452,6 +475,7 @@ class VelocityVerletIntegrator:
             _check(LIB.md_step_list(system.h, force_field.h, neighbour_list.h, self.dt, C.byref(pe), C.byref(r)))
             self.last_rebuilt = bool(r.value)
             neighbour_list.n = system.n
+        force_field.fetch_results()
         return pe.value
 
     def run(self, system: System, force_field: LennardJonesForceField, neighbour_list: NeighbourList, n_steps: int,
@@ -484,3 +508,102 @@ class VelocityVerletIntegrator:
                           _pd(w)))
         neighbour_list.n = system.n
         return pe, ke, w
+
+
+class Batch:
+    """Many independent replicas advanced together (md_batch_*): each replica is the reference's System with
+    NeighbourList(cutoff, skin, True), a deterministic LennardJonesForceField and VelocityVerletIntegrator, plus
+    an optional thermostat per replica; the reference has no batched class, so this stands for a loop over
+    systems. `systems` is a list of (pos (n, 4), box_length, vel (3, n) or None, mass (n,) or None) tuples."""
+
+    def __init__(self, systems, cutoff=2.5, skin=0.3, dt=0.005, epsilon=1.0, sigma=1.0, precision=PREC_FP64,
+                 thermostat="none", temperatures=None, seeds=None, rescale_every=10, bussi_tau=0.1,
+                 energy_every=0, chunk_steps=0, initial_capacity=0, device=0):
+        self.replicas = len(systems)
+        n = np.array([len(p) for p, *_ in systems], dtype=np.int64)
+        box = np.array([float(b) for _, b, *_ in systems])
+        pos = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.float64).reshape(-1, 4) for p, *_ in systems]))
+        vel = np.ascontiguousarray(np.concatenate([
+            (np.zeros(3 * len(p)) if v is None else np.asarray(v, dtype=np.float64).reshape(-1))
+            for p, _, v, *_ in systems]))
+        mass = np.ascontiguousarray(np.concatenate([
+            (np.ones(len(p)) if m is None else np.asarray(m, dtype=np.float64)) for p, _, _, m in systems]))
+        o = md_batch_options()
+        o.epsilon, o.sigma, o.cutoff, o.skin, o.dt = epsilon, sigma, cutoff, skin, dt
+        o.precision = precision
+        o.thermostat = {"none": 0, "rescale": 1, "bussi": 2}[thermostat]
+        o.rescale_every, o.bussi_tau = rescale_every, bussi_tau
+        o.energy_every, o.chunk_steps, o.initial_capacity = energy_every, chunk_steps, initial_capacity
+        temps = None if temperatures is None else np.ascontiguousarray(temperatures, dtype=np.float64)
+        sd = None if seeds is None else np.ascontiguousarray(seeds, dtype=np.uint64)
+        h = C.c_void_p()
+        _check(LIB.md_batch_create(device, self.replicas, n.ctypes.data_as(C.POINTER(C.c_int64)), _pd(box),
+                                   _pd(temps), _pu(sd), _pd(pos), _pd(vel), _pd(mass), C.byref(o), C.byref(h)))
+        self.h = h
+        self.n = n
+        self.box = box
+        self.energy_every = energy_every
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            LIB.md_batch_destroy(self.h)
+            self.h = None
+
+    def info(self) -> dict:
+        r, cap = C.c_int(), C.c_int()
+        atoms, launches = C.c_int64(), C.c_uint64()
+        _check(LIB.md_batch_info(self.h, C.byref(r), C.byref(atoms), C.byref(cap), C.byref(launches)))
+        return dict(replicas=r.value, atoms=atoms.value, capacity=cap.value, launches=launches.value)
+
+    def run(self, n_steps: int):
+        """n_steps steps of every replica; returns (pe, virial, ke) arrays of shape (n_steps // energy_every,
+        replicas) when energy_every > 0, else None."""
+        rows = n_steps // self.energy_every if self.energy_every > 0 else 0
+        if rows == 0:
+            _check(LIB.md_batch_run(self.h, n_steps, None, None, None))
+            return None
+        pe, w, ke = (np.zeros((rows, self.replicas)) for _ in range(3))
+        _check(LIB.md_batch_run(self.h, n_steps, _pd(pe), _pd(w), _pd(ke)))
+        return pe, w, ke
+
+    def energy(self):
+        """(pe, virial, ke, inside) arrays over replicas for the current state."""
+        out = [np.zeros(self.replicas) for _ in range(4)]
+        _check(LIB.md_batch_energy(self.h, *(_pd(a) for a in out)))
+        return tuple(out)
+
+    def download(self, replica: int) -> dict:
+        k = int(self.n[replica])
+        pos, vel, force, mass = np.zeros((k, 4)), np.zeros((3, k)), np.zeros((3, k)), np.zeros(k)
+        ids = np.zeros(k, dtype=np.uint64)
+        _check(LIB.md_batch_download(self.h, replica, _pd(pos), _pd(vel), _pd(force), _pd(mass), _pu(ids)))
+        return dict(pos=pos, vel=vel, force=force, mass=mass, ids=ids)
+
+    def state_hashes(self) -> np.ndarray:
+        h = np.zeros(self.replicas, dtype=np.uint64)
+        _check(LIB.md_batch_state_hash(self.h, _pu(h)))
+        return h
+
+    def rebuilds(self) -> np.ndarray:
+        r = np.zeros(self.replicas, dtype=np.uint64)
+        _check(LIB.md_batch_rebuilds(self.h, _pu(r)))
+        return r
+
+    def set_force_variant(self, variant: int):
+        _check(LIB.md_batch_set_force_variant(self.h, variant))
+
+    def force_variant(self) -> dict:
+        v, c, apb, tpa = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(LIB.md_batch_force_variant(self.h, C.byref(v), C.byref(c), C.byref(apb), C.byref(tpa)))
+        return dict(variant=v.value, count=c.value, particles_per_block=apb.value, threads_per_particle=tpa.value)
+
+    def time_forces(self, reps: int = 10) -> float:
+        ms = C.c_double()
+        _check(LIB.md_batch_time_forces(self.h, reps, C.byref(ms)))
+        return ms.value
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        _check(LIB.md_batch_stream(self.h, C.byref(p)))
+        return p.value or 0
+

@@ -10,6 +10,9 @@ all that the tests read.
 """
 from __future__ import annotations
 
+import gzip
+import hashlib
+import json
 import os
 import re
 import subprocess
@@ -139,14 +142,58 @@ def bussi(r: Reference):
     return dict(ke0=ke0, ke=np.array(ke), final_vel=st.vel, hash=s.hash())
 
 
+# md_sim command lines whose outputs the GPU md_sim must reproduce byte for byte (FP64, --deterministic) or
+# within tolerance (the default and --mixed force paths)
+MD_SIM_CASES = {
+    "nve_rescale": ["8", "--deterministic", "--skin", "0.3", "--temperature", "0.71", "--equil", "100", "--steps",
+                    "300", "--xyz-every", "100"],
+    "nvt_melt_rdf": ["6", "--deterministic", "--nvt", "--melt", "--seed", "7", "--equil", "60", "--steps", "200",
+                     "--density", "0.9", "--temperature", "1.2"],
+    "brute": ["5", "--brute", "--deterministic", "--equil", "20", "--steps", "60", "--dt", "0.004"],
+    "default_list": ["8", "--skin", "0.3", "--temperature", "0.71", "--equil", "50", "--steps", "200"],
+    "mixed": ["8", "--mixed", "--skin", "0.3", "--temperature", "0.71", "--equil", "50", "--steps", "200"],
+}
+
+
+def md_sim_case(binary: str, args: list[str], workdir: str) -> dict:
+    """Runs one md_sim command line with --csv/--rdf/--xyz outputs under `workdir`; returns its stdout (timing and
+    thread-count lines dropped), the RESULT fields that do not depend on timing, and the output files' text."""
+    files = {"csv": os.path.join(workdir, "run.csv"), "xyz": os.path.join(workdir, "run.xyz")}
+    extra = ["--csv", files["csv"], "--xyz", files["xyz"]]
+    if "--brute" not in args:
+        files["rdf"] = os.path.join(workdir, "run.rdf")
+        extra += ["--rdf", files["rdf"]]
+    out = subprocess.run([binary, *args, *extra], capture_output=True, text=True, check=True,
+                         env=dict(os.environ, OMP_NUM_THREADS="4")).stdout
+    result = dict(kv.split("=", 1) for kv in re.search(r"^RESULT (.*)$", out, re.M).group(1).split())
+    for k in ("threads", "seconds", "ms_per_step"):
+        result.pop(k)
+    table = [ln for ln in out.splitlines() if not ln.startswith(("N = ", "Production took", "RESULT"))]
+    texts = {k: open(f).read() for k, f in files.items()}
+    # The trajectory is kept as its digest and the head of its first frame
+    xyz = texts.pop("xyz")
+    texts["xyz_sha256"] = hashlib.sha256(xyz.encode()).hexdigest()
+    texts["xyz_head"] = "".join(xyz.splitlines(keepends=True)[:102])
+    return dict(stdout=table, result=result, files=texts)
+
+
+def md_sim_golden() -> dict:
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as d:
+        return {name: dict(args=args, **md_sim_case(REF_MD_SIM, args, d)) for name, args in MD_SIM_CASES.items()}
+
+
 def main():
     r = Reference()
     r.set_threads(4)
     np.savez_compressed(os.path.join(OUT, "config1.npz"), **config1(r))
     np.savez_compressed(os.path.join(OUT, "small_box.npz"), **small_box(r))
     np.savez_compressed(os.path.join(OUT, "bussi.npz"), **bussi(r))
+    with gzip.open(os.path.join(OUT, "md_sim.json.gz"), "wt") as f:
+        json.dump(md_sim_golden(), f)
     for f in sorted(os.listdir(OUT)):
-        if f.endswith(".npz"):
+        if f.endswith((".npz", ".gz")):
             print(f, os.path.getsize(os.path.join(OUT, f)))
 
 

@@ -72,3 +72,26 @@ def test_argument_errors_are_reported():
     assert e.value.name == "MD_ERR_INVALID"
     with pytest.raises(mdgpu.MDError):
         mdgpu.RadialDistribution(1.0, 0)
+
+
+def test_batch_geometry_and_option_errors():
+    """md_batch_create validates every replica before touching a device: the reference's geometry errors
+    (src/Forcefield.cpp:18-22, src/NeighbourList.cpp:57-59) per replica, then bad options."""
+    import mdgpu
+
+    a = mdgpu.lattice_constant(0.8442)
+    ok = (mdgpu.fcc_lattice(6, a), 6 * a, None, None)
+    small = (mdgpu.fcc_lattice(3, a), 3 * a, None, None)  # L = 5.04 < 2 (r_c + skin)
+    with pytest.raises(mdgpu.MDError) as e:
+        mdgpu.Batch([ok, small], cutoff=2.5, skin=0.3)
+    assert e.value.name == "MD_ERR_LIST_RADIUS" and "replica 1" in str(e.value)
+    with pytest.raises(mdgpu.MDError) as e:
+        mdgpu.Batch([small], cutoff=2.6, skin=0.1)
+    assert e.value.name == "MD_ERR_CUTOFF"
+    with pytest.raises(mdgpu.MDError) as e:
+        mdgpu.Batch([ok], thermostat="bussi", temperatures=[1.0])  # no seeds
+    assert e.value.name == "MD_ERR_INVALID"
+    if mdgpu.device_count() == 0:
+        with pytest.raises(mdgpu.MDError) as e:
+            mdgpu.Batch([ok])
+        assert e.value.name == "MD_ERR_NO_DEVICE"

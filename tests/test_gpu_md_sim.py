@@ -1,0 +1,85 @@
+"""The GPU md_sim (molecular-dynamics_b200/driver/md_sim.cpp over the drop-in classes) against the reference's
+md_sim (src/main.cpp) on the command lines in tests/golden/md_sim.json.gz.
+
+With --deterministic (and --brute) the FP64 path is bit-exact, so stdout tables, the RESULT line (timing fields
+aside), the CSV, the g(r) file and the XYZ trajectory must be identical byte for byte. The reference's default
+list path and its --mixed FP32 path sum in another order, so those are compared within tolerance."""
+from __future__ import annotations
+
+import gzip
+import hashlib
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+MD_SIM = os.path.join(ROOT, "molecular-dynamics_b200", "md_sim")
+GOLDEN = os.path.join(ROOT, "tests", "golden", "md_sim.json.gz")
+
+pytestmark = pytest.mark.gpu
+
+EXACT = ("nve_rescale", "nvt_melt_rdf", "brute")
+
+
+@pytest.fixture(scope="module")
+def golden(md):
+    subprocess.run(["make", "--no-print-directory", "-C", os.path.join(ROOT, "molecular-dynamics_b200", "dropin")],
+                   check=True)
+    with gzip.open(GOLDEN, "rt") as f:
+        return json.load(f)
+
+
+def run_md_sim(args, workdir):
+    files = {"csv": os.path.join(workdir, "run.csv"), "xyz": os.path.join(workdir, "run.xyz")}
+    extra = ["--csv", files["csv"], "--xyz", files["xyz"]]
+    if "--brute" not in args:
+        files["rdf"] = os.path.join(workdir, "run.rdf")
+        extra += ["--rdf", files["rdf"]]
+    r = subprocess.run([MD_SIM, *args, *extra], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    result = dict(kv.split("=", 1) for kv in re.search(r"^RESULT (.*)$", r.stdout, re.M).group(1).split())
+    for k in ("threads", "seconds", "ms_per_step"):
+        result.pop(k)
+    table = [ln for ln in r.stdout.splitlines() if not ln.startswith(("N = ", "Production took", "RESULT"))]
+    texts = {k: open(f).read() for k, f in files.items()}
+    xyz = texts.pop("xyz")
+    texts["xyz_sha256"] = hashlib.sha256(xyz.encode()).hexdigest()
+    texts["xyz_head"] = "".join(xyz.splitlines(keepends=True)[:102])
+    return dict(stdout=table, result=result, files=texts)
+
+
+def csv_columns(text):
+    rows = [ln.split(",") for ln in text.strip().splitlines()[1:]]
+    return np.array([[float(v) for i, v in enumerate(r) if i != 2] for r in rows])
+
+
+@pytest.mark.parametrize("case", EXACT)
+def test_md_sim_deterministic_outputs_identical(golden, tmp_path, case):
+    g = golden[case]
+    out = run_md_sim(g["args"], str(tmp_path))
+    assert out["result"] == g["result"]
+    assert out["stdout"] == g["stdout"]
+    for k in g["files"]:
+        assert out["files"][k] == g["files"][k], k
+
+
+# --mixed: the reference's float pair path (src/Forcefield.cpp:333-450) against FP32 pairs with fixed-point
+# sums; the virial, and with it the pressure, carries the largest float error of the columns
+@pytest.mark.parametrize("case,rtol", [("default_list", 1e-9), ("mixed", 5e-6)])
+def test_md_sim_reordered_paths_within_tolerance(golden, tmp_path, case, rtol):
+    """Per-step KE/N, PE/N, E/N, T and pressure against the reference run on the same command line."""
+    g = golden[case]
+    out = run_md_sim(g["args"], str(tmp_path))
+    ref, got = csv_columns(g["files"]["csv"]), csv_columns(out["files"]["csv"])
+    assert got.shape == ref.shape
+    assert np.array_equal(got[:, 0], ref[:, 0])
+    # columns: step, time, KE/N, PE/N, E/N, T, P, inside pairs; the CSV keeps 8 decimals
+    scale = np.abs(ref[:, 2:7]).max(axis=0)
+    err = np.abs(got[:, 2:7] - ref[:, 2:7]).max(axis=0) / scale
+    assert (err <= rtol + 1e-8).all(), err
+    assert abs(float(out["result"]["mean_T"]) - float(g["result"]["mean_T"])) <= 1e-5
+    assert out["result"]["rebuilds"] == g["result"]["rebuilds"]
