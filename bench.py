@@ -38,6 +38,8 @@ for _p in (ROOT, PKG):
 
 METRIC = "atom-steps/s at N=4M, FP32+fixed-pt vs FP64 GPU at <=1e-6 rel force err; %roofline"
 FALLBACK_HBM_GBS = 6650.0
+# precision name -> (md_precision value, arithmetic of the pair path)
+PRECISIONS = {"fp32fx": (1, "f32+i64"), "fp32": (2, "f32"), "fp64": (0, "f64"), "fx64": (3, "i32+f64+i64")}
 
 
 def args_parse():
@@ -50,8 +52,10 @@ def args_parse():
     p.add_argument("--density", type=float, default=0.8442)
     p.add_argument("--temperature", type=float, default=0.71)
     p.add_argument("--equil", type=int, default=200)
-    p.add_argument("--precision", choices=["fp32fx", "fp32", "fp64"], default="fp32fx")
+    p.add_argument("--precision", choices=list(PRECISIONS), default="fp32fx")
     p.add_argument("--fp64-steps", type=int, default=100, help="steps of the FP64 comparison run (0: skip)")
+    p.add_argument("--side-steps", type=int, default=300,
+                   help="steps of the runs of the other float precisions on the same state (0: skip)")
     p.add_argument("--cpu-steps", type=int, default=3, help="reference steps in the cpu_baseline sample (0: skip)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--sweep", choices=["precision"], default=None,
@@ -237,15 +241,17 @@ def force_errors(md, s, nl) -> dict:
     w64 = ff64.virial
     f64 = s.forces()
     out = {}
-    for name, prec in (("fp32fx", md.PREC_FP32FX), ("fp32", md.PREC_FP32)):
-        ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)
+    for name in ("fp32fx", "fp32", "fx64"):
+        ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=PRECISIONS[name][0])
         pe = ff.compute_forces(s, nl)
         f = s.forces()
         d = np.linalg.norm(f - f64, axis=0)
         mag = np.linalg.norm(f64, axis=0)
         rel = d / np.maximum(mag, 1e-300)
+        rms = float(np.sqrt((mag ** 2).mean()))
         out[name] = {"max_abs_dF_over_max_F": float(np.abs(f - f64).max() / np.abs(f64).max()),
-                     "rms_dF_over_rms_F": float(np.sqrt((d ** 2).mean() / (mag ** 2).mean())),
+                     "rms_dF_over_rms_F": float(np.sqrt((d ** 2).mean()) / rms),
+                     "max_particle_dF_over_rms_F": float(d.max() / rms),
                      "per_particle_rel_p50": float(np.percentile(rel, 50)),
                      "per_particle_rel_p99": float(np.percentile(rel, 99)),
                      "per_particle_rel_max": float(rel.max()),
@@ -272,7 +278,7 @@ def run_gpu_arm(a):
 
     import mdgpu as md
 
-    prec = {"fp32fx": md.PREC_FP32FX, "fp32": md.PREC_FP32, "fp64": md.PREC_FP64}[a.precision]
+    prec = PRECISIONS[a.precision][0]
     n = 4 * a.cells ** 3
     dt = 0.005
     s = md.fcc_system(a.cells, a.density, a.temperature, seed=42 + rank, device=local)
@@ -318,30 +324,36 @@ def run_gpu_arm(a):
     e0 = pe[0] + ke[0]
     drift = float(np.abs((pe + ke - e0) / e0).max())
 
-    # FP64 path on a copy of the same state (bit-identical to the reference's deterministic mode)
-    fp64 = None
-    if a.fp64_steps and rank == 0:
+    # The FP64 path (bit-identical to the reference's deterministic mode) and the other float precisions on
+    # copies of the same state
+    def side_run(precision: int, steps: int) -> dict:
         st = s.download()
-        s64 = md.System.from_arrays(st["pos"], s.box, vel=st["vel"], force=st["force"], device=local)
-        nl64 = md.NeighbourList(2.5, 0.3)
-        nl64.build(s64)
-        ff64 = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=md.PREC_FP64)
-        ff64.compute_forces(s64, nl64)
-        integ.run(s64, ff64, nl64, 5)
-        st64 = torch.cuda.ExternalStream(s64.stream)
+        s2 = md.System.from_arrays(st["pos"], s.box, vel=st["vel"], force=st["force"], device=local)
+        nl2 = md.NeighbourList(2.5, 0.3)
+        nl2.build(s2)
+        ff2 = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=precision)
+        ff2.compute_forces(s2, nl2)
+        integ.run(s2, ff2, nl2, 5)
+        st2 = torch.cuda.ExternalStream(s2.stream)
         e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s64.synchronize()
-        s64.profile(True)
-        e0_.record(st64)
-        pe64, ke64, _ = integ.run(s64, ff64, nl64, a.fp64_steps)
-        e1_.record(st64)
+        s2.synchronize()
+        s2.profile(True)
+        e0_.record(st2)
+        pe2, ke2, _ = integ.run(s2, ff2, nl2, steps)
+        e1_.record(st2)
         e1_.synchronize()
-        ms64 = e0_.elapsed_time(e1_)
-        f64_ms, f64_n = s64.profile_read()
-        fp64 = {"value": n * a.fp64_steps / (ms64 / 1e3), "steps": a.fp64_steps, "ms_per_step": ms64 / a.fp64_steps,
-                "force_kernel_ms": f64_ms / max(f64_n, 1),
-                "max_drift": float(np.abs((pe64 + ke64 - pe64[0] - ke64[0]) / (pe64[0] + ke64[0])).max())}
-        del s64, nl64, ff64
+        ms2 = e0_.elapsed_time(e1_)
+        f_ms, f_n = s2.profile_read()
+        return {"value": n * steps / (ms2 / 1e3), "steps": steps, "ms_per_step": ms2 / steps,
+                "force_kernel_ms": f_ms / max(f_n, 1),
+                "max_drift": float(np.abs((pe2 + ke2 - pe2[0] - ke2[0]) / (pe2[0] + ke2[0])).max())}
+
+    fp64 = side_run(md.PREC_FP64, a.fp64_steps) if a.fp64_steps and rank == 0 else None
+    others = {}
+    if a.side_steps and rank == 0:
+        for name in ("fp32fx", "fx64", "fp32"):
+            if name != a.precision:
+                others[name] = side_run(PRECISIONS[name][0], a.side_steps)
 
     # End to end through the public C-ABI with host buffers: pinned host state -> device, list build,
     # initial forces, K steps returning per-step PE/KE/virial, final positions and velocities -> host.
@@ -402,15 +414,17 @@ def run_gpu_arm(a):
     value = replica_throughput(world, n, a.steps, ms)
     line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": {"fp32fx": "f32+i64", "fp32": "f32", "fp64": "f64"}[a.precision],
+            "vs_baseline": None, "dtype": PRECISIONS[a.precision][1],
             "data": "synthetic", "config": workload(a),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None if tpa is None else tpa * n,
-                         "kernel": "k_force_fp32", "kernel_ms": kernel_s * 1e3,
+                         "kernel": {"fp64": "k_force_fp64", "fx64": "k_force_fx64_rows"}.get(a.precision, "k_force_fp32"),
+                         "kernel_ms": kernel_s * 1e3,
                          "algorithmic_bytes_per_atom": bytes_per_atom, "peak_source": peak_src},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
             "rebuilds": rebuilds, "half_list_pairs": pairs, "max_energy_drift": drift,
             "fp64": fp64, "speedup_vs_fp64": None if fp64 is None else value / world / fp64["value"],
+            "other_precisions": others,
             "force_error_vs_fp64": errors}
     print(json.dumps(line), flush=True)
     if dist:
@@ -445,7 +459,8 @@ def precision_sweep(cells=40, densities=(0.5, 0.8442, 1.0), temperatures=(0.71, 
             start = s.download()
             vol = s.box ** 3
             runs = {}
-            for name, prec in (("fp64", md.PREC_FP64), ("fp32fx", md.PREC_FP32FX), ("fp32", md.PREC_FP32)):
+            for name in ("fp64", "fp32fx", "fp32", "fx64"):
+                prec = PRECISIONS[name][0]
                 r = md.System.from_arrays(start["pos"], s.box, vel=start["vel"], force=start["force"], device=device)
                 rl = md.NeighbourList(2.5, 0.3)
                 rf = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)

@@ -38,7 +38,9 @@ typedef enum md_status {
 typedef enum md_precision {
     MD_PREC_FP64 = 0,   /* double throughout, bit-identical to the reference's deterministic path */
     MD_PREC_FP32FX = 1, /* float pair arithmetic, 64-bit fixed-point force accumulation */
-    MD_PREC_FP32 = 2    /* float pair arithmetic, float accumulation */
+    MD_PREC_FP32 = 2,   /* float pair arithmetic, float accumulation */
+    MD_PREC_FX64 = 3    /* exact separations from 32-bit fixed-point frames, double pair terms, 64-bit
+                           fixed-point accumulation */
 } md_precision;
 
 typedef struct md_system md_system;         /* System (include/System.hpp:12) */

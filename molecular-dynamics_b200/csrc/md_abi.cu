@@ -7,6 +7,7 @@
 #include "md_common.cuh"
 #include "md_fp32.cuh"
 #include "md_fp64.cuh"
+#include "md_fx64.cuh"
 #include "md_nlist.cuh"
 #include "md_scan.cuh"
 #include "md_tiles.cuh"
@@ -147,10 +148,11 @@ struct md_nlist {
     DevBuf<long long> half_off, rev_off, tiles;
     DevBuf<double4> ref_pos;
     DevBuf<float4> frames;  // per-particle float coordinates for the float kernels (n + 1, sentinel last)
+    DevBuf<int4> iframes;   // fixed-point frames of MD_PREC_FX64 (n)
     bool use_tiles = false; // shared-memory tile kernels (3+ cells per side and tiles that fit)
     TileGeom tiles_geom{};
-    int variant[3] = {-1, -1, -1};  // force kernel per precision (0 global gathers, 1 tile; -1 untuned)
-    int pinned[3] = {-1, -1, -1};   // set by md_nlist_set_force_variant
+    int variant[4] = {-1, -1, -1, -1};  // force kernel per precision (0 global gathers, 1 tile; -1 untuned)
+    int pinned[4] = {-1, -1, -1, -1};   // set by md_nlist_set_force_variant
     int rebuilds = 0;
     uint64_t pairs = 0;
     bool built = false;
@@ -603,7 +605,7 @@ md_status kick_drift_async(md_system* s, md_nlist* nl, double dt, bool check_ski
 // rebuilt. Afterwards the float frames match the positions whenever the list uses tiles.
 md_status drift_and_update(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, bool* rebuilt) {
     const bool current = nlist_current(nl, s);
-    const bool frames = current && nl->use_tiles && ff->precision != MD_PREC_FP64;
+    const bool frames = current && nl->use_tiles && (ff->precision == MD_PREC_FP32FX || ff->precision == MD_PREC_FP32);
     MD_TRY(kick_drift_async(s, nl, dt, current, frames));
     bool stale = true;
     if (current) {
@@ -1047,7 +1049,8 @@ md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_c
 }
 
 md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant) {
-    if (!nl || precision < MD_PREC_FP64 || precision > MD_PREC_FP32 || variant < -1 || variant > 1)
+    if (!nl || precision < MD_PREC_FP64 || precision > MD_PREC_FX64 || variant < -1 || variant > 1 ||
+        (precision == MD_PREC_FX64 && variant == 1))
         return fail(MD_ERR_INVALID, "md_nlist_set_force_variant: bad arguments");
     nl->pinned[precision] = variant;
     nl->variant[precision] = -1;
@@ -1055,7 +1058,7 @@ md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant) {
 }
 
 md_status md_nlist_force_variant(const md_nlist* nl, int precision, int* variant) {
-    if (!nl || !variant || precision < MD_PREC_FP64 || precision > MD_PREC_FP32)
+    if (!nl || !variant || precision < MD_PREC_FP64 || precision > MD_PREC_FX64)
         return fail(MD_ERR_INVALID, "md_nlist_force_variant: bad arguments");
     *variant = nl->variant[precision];
     return MD_OK;
@@ -1147,7 +1150,7 @@ md_status md_forcefield_shift(const md_forcefield* ff, double* shift) {
 }
 
 md_status md_forcefield_set_precision(md_forcefield* ff, int precision) {
-    if (!ff || precision < MD_PREC_FP64 || precision > MD_PREC_FP32) return fail(MD_ERR_INVALID, "bad precision");
+    if (!ff || precision < MD_PREC_FP64 || precision > MD_PREC_FX64) return fail(MD_ERR_INVALID, "bad precision");
     ff->precision = precision;
     return MD_OK;
 }

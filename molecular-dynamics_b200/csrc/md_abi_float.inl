@@ -42,9 +42,80 @@ md_status frames_async(md_system* s, md_nlist* nl) {
     return MD_OK;
 }
 
+Fx64LJ fx64_lj(const md_forcefield* ff) {
+    Fx64LJ f{};
+    f.lj = ff->lj;
+    f.eps48 = 2.0 * ff->lj.eps24;
+    // the fixed-point separation is exact to ~4e-9, so r^2 is within ~3e-8 of the reference's
+    f.band = 1e-6 * ff->lj.rc2;
+    return f;
+}
+
+FixedOffsets fixed_offsets(const md_nlist* nl, const md_system* s) {
+    FixedOffsets o{};
+    const int cellq = static_cast<int>(std::llrint(cell_side(nl, s) * kFrameScale));
+    for (int code = 0; code < 27; ++code) {
+        const int d[3] = {code / 9 - 1, (code / 3) % 3 - 1, code % 3 - 1};
+        o.off[code] = make_int4(-d[0] * cellq, -d[1] * cellq, -d[2] * cellq, 0);
+    }
+    return o;
+}
+
+// MD_PREC_FX64 list forces: fixed-point frames of the current positions, then the global-gather kernel (or the
+// small-box kernel under 3 cells per side); the closing kick and kinetic energy are fused as in the float modes
+md_status forces_list_fx64_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt,
+                                 bool* fused_ke) {
+    const int n = static_cast<int>(s->n);
+    const bool kick = kick_dt > 0.0;
+    const Fx64LJ lj = fx64_lj(ff);
+    MD_CUDA(ff->fx_acc.reserve(4));
+    if (want_energy || kick) MD_CUDA(cudaMemsetAsync(ff->fx_acc.p, 0, 4 * sizeof(long long), s->stream));
+    auto* acc = reinterpret_cast<unsigned long long*>(ff->fx_acc.p);
+    nl->variant[MD_PREC_FX64] = 0;
+    if (n > 0) {
+        const unsigned g = blocks_for(n, 128);
+        const KickArgs ka{kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
+        if (nl->use_cells) {
+            MD_CUDA(nl->iframes.reserve(n));
+            k_frames_fixed<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(s->pos.p, n, nl->cell_sorted.p,
+                                                                               nl->grid.ncps, cell_side(nl, s), s->box,
+                                                                               nl->iframes.p);
+            MD_CHECK_LAUNCH();
+            const FixedOffsets offs = fixed_offsets(nl, s);
+            MD_TRY(profile_mark(s));
+            if (want_energy)
+                k_force_fx64_rows<true><<<g, 128, 0, s->stream>>>(nl->iframes.p, s->pos.p, n, s->box, lj, offs, nl->rows.p,
+                                                                  nl->cap, nl->counts.p, s->force.p, acc, ka);
+            else
+                k_force_fx64_rows<false><<<g, 128, 0, s->stream>>>(nl->iframes.p, s->pos.p, n, s->box, lj, offs,
+                                                                   nl->rows.p, nl->cap, nl->counts.p, s->force.p, acc, ka);
+        } else {
+            MD_TRY(profile_mark(s));
+            if (want_energy)
+                k_force_fx64_small<true><<<g, 128, 0, s->stream>>>(s->pos.p, n, s->box, lj, nl->rows.p, nl->cap,
+                                                                   nl->counts.p, s->force.p, acc, ka);
+            else
+                k_force_fx64_small<false><<<g, 128, 0, s->stream>>>(s->pos.p, n, s->box, lj, nl->rows.p, nl->cap,
+                                                                    nl->counts.p, s->force.p, acc, ka);
+        }
+        MD_CHECK_LAUNCH();
+        MD_TRY(profile_mark(s));
+    }
+    const bool ke_fused = kick && n > 0;
+    if (want_energy || ke_fused) {
+        k_finish_float_energy<<<1, 1, 0, s->stream>>>(acc, ff->out.p, ff->inside_count.p,
+                                                      ke_fused ? s->scal.p + kScalKE : nullptr, 1.0 / kKineticScale,
+                                                      kEnergyUnit64);
+        MD_CHECK_LAUNCH();
+    }
+    if (fused_ke) *fused_ke = ke_fused;
+    return MD_OK;
+}
+
 // See forces_list_async. Every float kernel fuses the closing kick with a fixed-point kinetic energy.
 md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt,
                                   bool frames_fresh, bool* fused_ke) {
+    if (ff->precision == MD_PREC_FX64) return forces_list_fx64_async(ff, s, nl, want_energy, kick_dt, fused_ke);
     const int n = static_cast<int>(s->n);
     const bool fixed = ff->precision == MD_PREC_FP32FX;
     const bool kick = kick_dt > 0.0;

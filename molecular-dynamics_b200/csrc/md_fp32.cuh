@@ -23,8 +23,10 @@ namespace md {
 
 constexpr float kForceScale = 4294967296.0f;        // 2^32: fixed-point units per unit force
 constexpr double kForceUnit = 1.0 / 4294967296.0;
-constexpr float kEnergyScale = 16777216.0f;         // 2^24 for energy and virial sums
+constexpr float kEnergyScale = 16777216.0f;         // 2^24 for energy and virial sums of float groups
 constexpr double kEnergyUnit = 1.0 / 16777216.0;
+constexpr double kEnergyScale64 = 1073741824.0;     // 2^30 for energy and virial sums of double groups (FX64)
+constexpr double kEnergyUnit64 = 1.0 / 1073741824.0;
 constexpr double kKineticScale = 4294967296.0;      // 2^32: fixed-point units of the fused kinetic energy
 constexpr float kSentinelCoord = 1.0e15f;           // frame of the sentinel particle: never inside the cutoff
 
@@ -111,6 +113,18 @@ struct FloatAcc {
         if (kEnergy) {
             e_fx += __float2ll_rn(ge * kEnergyScale);
             w_fx += __float2ll_rn(gw * kEnergyScale);
+        }
+    }
+    // A group summed in double (MD_PREC_FX64): the same fixed-point units, rounded from double
+    __device__ __forceinline__ void add_group(double gx, double gy, double gz, double ge, double gw, long long& e_fx,
+                                              long long& w_fx) {
+        static_assert(kFixed, "double groups accumulate in fixed point");
+        ax += __double2ll_rn(dmul(gx, static_cast<double>(kForceScale)));
+        ay += __double2ll_rn(dmul(gy, static_cast<double>(kForceScale)));
+        az += __double2ll_rn(dmul(gz, static_cast<double>(kForceScale)));
+        if (kEnergy) {
+            e_fx += __double2ll_rn(dmul(ge, kEnergyScale64));
+            w_fx += __double2ll_rn(dmul(gw, kEnergyScale64));
         }
     }
     // Write the force (double, component-major) and apply the fused closing kick; returns the particle's
@@ -255,14 +269,14 @@ __global__ void k_force_fp32_small(const double4* __restrict__ pos, int n, Box b
     if (kEnergy || kick.vel) flush_sums(e_fx, w_fx, ins, k_fx, acc);
 }
 
-// Converts the fixed-point sums to doubles: (pe, virial) with the double-counted pairs halved into out[0..1],
-// the inside count (halved, an integer) into *inside, and, when ke_out is set, the fused kinetic energy
-// (2^-32 units) into *ke_out.
+// Converts the fixed-point sums to doubles: (pe, virial) in `energy_unit`s with the double-counted pairs halved
+// into out[0..1], the inside count (halved, an integer) into *inside, and, when ke_out is set, the fused kinetic
+// energy (2^-32 units) into *ke_out.
 __global__ void k_finish_float_energy(const unsigned long long* __restrict__ acc, double* __restrict__ out,
                                       unsigned long long* __restrict__ inside, double* __restrict__ ke_out,
-                                      double kinetic_unit) {
-    out[0] = 0.5 * static_cast<double>(static_cast<long long>(acc[0])) * kEnergyUnit;
-    out[1] = 0.5 * static_cast<double>(static_cast<long long>(acc[1])) * kEnergyUnit;
+                                      double kinetic_unit, double energy_unit = kEnergyUnit) {
+    out[0] = 0.5 * static_cast<double>(static_cast<long long>(acc[0])) * energy_unit;
+    out[1] = 0.5 * static_cast<double>(static_cast<long long>(acc[1])) * energy_unit;
     *inside = acc[2] / 2;
     if (ke_out) *ke_out = static_cast<double>(static_cast<long long>(acc[3])) * kinetic_unit;
 }

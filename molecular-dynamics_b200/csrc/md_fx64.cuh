@@ -1,0 +1,158 @@
+// MD_PREC_FX64: exact separations from 32-bit fixed-point frames, pair terms in double, 64-bit fixed-point
+// force sums. The float modes lose most of their accuracy to the rounding of the separation (the force goes
+// as r^-14, so a relative error e of r becomes about 14 e of the force); here the separation of a pair is an
+// integer difference of frames in units of 2^-28 (exact, wrapping modulo 2^32 like the hardware adds) and only
+// its conversion to double rounds, so the per-particle force error against the FP64 path falls from about
+// 1e-6 to about 2e-8 of the force. Frames are still gathered as 16 bytes per neighbour.
+#pragma once
+
+#include "md_common.cuh"
+#include "md_fp32.cuh"
+
+namespace md {
+
+constexpr double kFrameScale = 268435456.0;  // 2^28 fixed-point frame units per unit length
+constexpr double kFrameUnit = 1.0 / 268435456.0;
+
+// frame_of in fixed point: round(q * 2^28) per component (|q| stays below a cell plus half the skin, far
+// inside the int32 range)
+__device__ __forceinline__ int4 fixed_frame_of(const double4& p, int c, int ncps, double cell, const Box& box) {
+    const int cx = c / (ncps * ncps), cy = (c / ncps) % ncps, cz = c % ncps;
+    double d[3] = {dsub(p.x, dmul(cx + 0.5, cell)), dsub(p.y, dmul(cy + 0.5, cell)), dsub(p.z, dmul(cz + 0.5, cell))};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d[k] = dsub(d[k], dmul(box.L, rint(dmul(d[k], box.invL))));
+    return make_int4(__double2int_rn(dmul(d[0], kFrameScale)), __double2int_rn(dmul(d[1], kFrameScale)),
+                     __double2int_rn(dmul(d[2], kFrameScale)), 0);
+}
+
+__global__ void k_frames_fixed(const double4* __restrict__ pos, int n, const int* __restrict__ cell_sorted, int ncps,
+                               double cell, Box box, int4* __restrict__ frames) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    frames[i] = fixed_frame_of(pos[i], cell_sorted[i], ncps, cell, box);
+}
+
+// -d * cell for the 27 codes in frame units (zero for the others); cellq = round(cell * 2^28) on the host
+struct FixedOffsets {
+    int4 off[32];
+};
+
+struct Fx64LJ {
+    LJ lj;
+    double eps48;  // 48 eps
+    double band;   // |r^2 - r_c^2| below this: decide inside/outside with the reference's exact test
+};
+
+// Separation of a row entry from fixed-point frames: (q_i - q_j) + offset in wrapping 32-bit arithmetic, then
+// exactly scaled to double; returns r^2
+__device__ __forceinline__ double fixed_separation(const int4& qi, const int4& qj, const int4& o, double& dx, double& dy,
+                                                   double& dz) {
+    const int sx = static_cast<int>(static_cast<unsigned>(qi.x) - static_cast<unsigned>(qj.x) + static_cast<unsigned>(o.x));
+    const int sy = static_cast<int>(static_cast<unsigned>(qi.y) - static_cast<unsigned>(qj.y) + static_cast<unsigned>(o.y));
+    const int sz = static_cast<int>(static_cast<unsigned>(qi.z) - static_cast<unsigned>(qj.z) + static_cast<unsigned>(o.z));
+    dx = dmul(__int2double_rn(sx), kFrameUnit);
+    dy = dmul(__int2double_rn(sy), kFrameUnit);
+    dz = dmul(__int2double_rn(sz), kFrameUnit);
+    return __fma_rn(dx, dx, __fma_rn(dy, dy, dmul(dz, dz)));
+}
+
+// One pair's terms in double with a pinned operation sequence: 1/r^2 from the float reciprocal refined by two
+// Newton steps, then F/r = (48 eps sr6 - 24 eps) sr6 / r^2 and E = 4 eps sr6 (sr6 - 1) - shift
+template <bool kEnergy>
+__device__ __forceinline__ void fx64_pair(double dx, double dy, double dz, bool in, double r2, const Fx64LJ& p,
+                                          double& gx, double& gy, double& gz, double& ge, double& gw,
+                                          unsigned long long& ins) {
+    double inv = static_cast<double>(__frcp_rn(__double2float_rn(r2)));
+    inv = __fma_rn(inv, __fma_rn(-r2, inv, 1.0), inv);
+    inv = __fma_rn(inv, __fma_rn(-r2, inv, 1.0), inv);
+    const double sr2 = dmul(p.lj.sig2, inv);
+    const double sr6 = dmul(dmul(sr2, sr2), sr2);
+    double fr = dmul(dmul(__fma_rn(p.eps48, sr6, -p.lj.eps24), sr6), inv);
+    fr = in ? fr : 0.0;
+    gx = __fma_rn(fr, dx, gx);
+    gy = __fma_rn(fr, dy, gy);
+    gz = __fma_rn(fr, dz, gz);
+    if (kEnergy) {
+        const double en = __fma_rn(dmul(p.lj.eps4, sr6), dsub(sr6, 1.0), -p.lj.shift);
+        ge = dadd(ge, in ? en : 0.0);
+        gw = __fma_rn(fr, r2, gw);
+        ins += in ? 1u : 0u;
+    }
+}
+
+// Thread per particle over its row (the layout of k_force_fp32_rows), frames gathered from global memory. Row
+// padding entries carry code 31 and are masked.
+template <bool kEnergy>
+__global__ void __launch_bounds__(128) k_force_fx64_rows(const int4* __restrict__ frames, const double4* __restrict__ pos,
+                                                         int n, Box box, Fx64LJ lj, FixedOffsets offs,
+                                                         const uint32_t* __restrict__ rows, int cap,
+                                                         const int2* __restrict__ counts, double* __restrict__ force,
+                                                         unsigned long long* __restrict__ acc, KickArgs kick) {
+    __shared__ int4 s_off[32];
+    if (threadIdx.x < 32) s_off[threadIdx.x] = offs.off[threadIdx.x];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    long long e_fx = 0, w_fx = 0, k_fx = 0;
+    unsigned long long ins = 0;
+    if (i < n) {
+        const int4 qi = frames[i];
+        const int2 c = counts[i];
+        const int groups = (c.x + c.y + 7) >> 3;
+        FloatAcc<true, kEnergy> a;
+        for (int g = 0; g < groups; ++g) {
+            const uint4 e0 = row_quad(rows, i, 2 * g, cap);
+            const uint4 e1 = row_quad(rows, i, 2 * g + 1, cap);
+            const uint32_t ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+            double gx = 0.0, gy = 0.0, gz = 0.0, ge = 0.0, gw = 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const uint32_t e = ent[u];
+                const uint32_t code = e >> kCodeShift;
+                // the sentinel's index is n: read particle 0's frame instead (masked below)
+                const int j = code == kSentinelCode ? 0 : static_cast<int>(e & kIndexMask);
+                double dx, dy, dz;
+                const double r2 = fixed_separation(qi, frames[j], s_off[code], dx, dy, dz);
+                bool in = code != kSentinelCode && r2 < lj.lj.rc2;
+                if (code != kSentinelCode && fabs(dsub(r2, lj.lj.rc2)) < lj.band)
+                    in = exact_inside(pos[i], pos[j], box, lj.lj.rc2);
+                fx64_pair<kEnergy>(dx, dy, dz, in, code == kSentinelCode ? 1.0 : r2, lj, gx, gy, gz, ge, gw, ins);
+            }
+            a.add_group(gx, gy, gz, ge, gw, e_fx, w_fx);
+        }
+        k_fx = a.finish(i, n, force, kick);
+    }
+    if (kEnergy || kick.vel) flush_sums(e_fx, w_fx, ins, k_fx, acc);
+}
+
+// Boxes under 3 cells per side: separations from the double positions with the reference's minimum image
+// (as k_force_fp32_small), the same double pair terms and fixed-point sums
+template <bool kEnergy>
+__global__ void k_force_fx64_small(const double4* __restrict__ pos, int n, Box box, Fx64LJ lj,
+                                   const uint32_t* __restrict__ rows, int cap, const int2* __restrict__ counts,
+                                   double* __restrict__ force, unsigned long long* __restrict__ acc, KickArgs kick) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    long long e_fx = 0, w_fx = 0, k_fx = 0;
+    unsigned long long ins = 0;
+    if (i < n) {
+        const double4 pi = pos[i];
+        const int2 c = counts[i];
+        const int m = c.x + c.y;
+        FloatAcc<true, kEnergy> a;
+        for (int g0 = 0; g0 < m; g0 += 8) {
+            double gx = 0.0, gy = 0.0, gz = 0.0, ge = 0.0, gw = 0.0;
+            for (int s = g0; s < g0 + 8 && s < m; ++s) {
+                const double4 pj = pos[rows[row_index(i, s, cap)] & kIndexMask];
+                const double dx = min_image(dsub(pi.x, pj.x), box);
+                const double dy = min_image(dsub(pi.y, pj.y), box);
+                const double dz = min_image(dsub(pi.z, pj.z), box);
+                const double r2 = norm2(dx, dy, dz);
+                fx64_pair<kEnergy>(dx, dy, dz, r2 < lj.lj.rc2, r2, lj, gx, gy, gz, ge, gw, ins);
+            }
+            a.add_group(gx, gy, gz, ge, gw, e_fx, w_fx);
+        }
+        k_fx = a.finish(i, n, force, kick);
+    }
+    if (kEnergy || kick.vel) flush_sums(e_fx, w_fx, ins, k_fx, acc);
+}
+
+}  // namespace md

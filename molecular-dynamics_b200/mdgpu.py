@@ -17,7 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmdgpu.so")
 
-PREC_FP64, PREC_FP32FX, PREC_FP32 = 0, 1, 2
+PREC_FP64, PREC_FP32FX, PREC_FP32, PREC_FX64 = 0, 1, 2, 3
 _ERRORS = {1: "MD_ERR_INVALID", 2: "MD_ERR_CUTOFF", 3: "MD_ERR_LIST_RADIUS", 4: "MD_ERR_NO_REVERSE_INDEX",
            5: "MD_ERR_CAPACITY", 6: "MD_ERR_CUDA", 7: "MD_ERR_NO_DEVICE", 8: "MD_ERR_STATE", 9: "MD_ERR_TIMEOUT"}
 

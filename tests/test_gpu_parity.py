@@ -234,13 +234,45 @@ def test_total_force_and_momentum(md, golden):
     assert np.all(np.abs(p) < 1e-10)
 
 
-@pytest.mark.parametrize("prec", ["fp64", "fp32fx", "fp32"])
+@pytest.mark.parametrize("cells,density", [(8, 0.8442), (6, 0.5), (20, 1.0)])
+def test_fx64_per_particle_force_error(md, golden, cells, density):
+    """MD_PREC_FX64 (exact fixed-point separations, double pair terms): every particle's force within 1e-6 of
+    the rms force of the FP64 path, 99 % of particles within 1e-6 of their own force, PE and virial within 1e-9,
+    the same inside count, bit-identical repeats. Liquid states (config 1's after 1000 steps, and melted
+    boxes), plus the FCC lattice start."""
+    if cells == 8:
+        s, nl = liquid(md, golden)
+    else:
+        s = md.fcc_system(cells, density, 2.0, seed=5)
+        nl = md.NeighbourList(2.5, 0.3)
+        nl.build(s)
+        warm = md.LennardJonesForceField(1.0, 1.0, 2.5)
+        warm.compute_forces(s, nl)
+        md.VelocityVerletIntegrator(0.005).run(s, warm, nl, 300, record=False)
+    ff = md.LennardJonesForceField(1.0, 1.0, 2.5)
+    pe64 = ff.compute_forces(s, nl)
+    f64, w64, ins64 = s.forces(), ff.virial, ff.inside_pairs
+    ff.set_precision(md.PREC_FX64)
+    pe = ff.compute_forces(s, nl)
+    f = s.forces()
+    d = np.linalg.norm(f - f64, axis=0)
+    mag = np.linalg.norm(f64, axis=0)
+    rms = np.sqrt((mag ** 2).mean())
+    assert d.max() <= 1e-6 * rms, d.max() / rms
+    assert (d <= 1e-6 * mag).mean() >= 0.99, (d <= 1e-6 * mag).mean()
+    assert abs(pe - pe64) <= 1e-9 * abs(pe64) and abs(ff.virial - w64) <= 1e-9 * abs(w64)
+    assert ff.inside_pairs == ins64
+    assert ff.compute_forces(s, nl) == pe and np.array_equal(s.forces(), f)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32fx", "fp32", "fx64"])
 def test_nve_energy_drift(md, golden, prec):
     """tests/test_dynamics.cpp:40-56 and tests/test_forcefield.cpp:151-167: |dE/E0| < 3e-4 over 2000 steps
     with more than one rebuild, starting from a melted liquid."""
     s, nl = liquid(md, golden)
     ff = md.LennardJonesForceField(1.0, 1.0, C1["rc"],
-                                   precision={"fp64": md.PREC_FP64, "fp32fx": md.PREC_FP32FX, "fp32": md.PREC_FP32}[prec])
+                                   precision={"fp64": md.PREC_FP64, "fp32fx": md.PREC_FP32FX, "fp32": md.PREC_FP32,
+                                              "fx64": md.PREC_FX64}[prec])
     pe0 = ff.compute_forces(s, nl)
     e0 = s.kinetic_energy() + pe0
     integ = md.VelocityVerletIntegrator(C1["dt"])
