@@ -139,10 +139,11 @@ md_status md_nlist_update(md_nlist* nl, md_system* s, int* rebuilt);
 /* getPairCount, getRebuildCount, the cell grid side of the last build, hasReverseIndex. Any may be NULL. */
 md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_count, int* cells_per_side,
                         int* reverse_index);
-/* Force kernel choice for one precision: -1 autotunes (the first force call of the list times the global-gather
- * and the shared-memory tile kernels and keeps the faster), 0 pins global gathers, 1 pins the tile kernel
- * (used only while the list has tiles). Every variant gives the same bits. md_nlist_force_variant reports the
- * variant in use (-1 until the first force call). */
+/* Force kernel choice for one precision: -1 autotunes (the first force call of the list times every
+ * available variant and keeps the fastest), 0 pins global gathers, 1 pins the shared-memory tile kernel (used
+ * only while the list has tiles; FP64 and the float modes), 2 pins global gathers with the rows prefetched a
+ * group ahead (float modes). Every variant gives the same bits. md_nlist_force_variant reports the variant in
+ * use (-1 until the first force call). */
 md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant);
 md_status md_nlist_force_variant(const md_nlist* nl, int precision, int* variant);
 /* Layout of the last build (diagnostics): whether the shared-memory tile kernels are in use, the segment
@@ -271,6 +272,34 @@ md_status md_batch_force_variant(const md_batch* b, int* variant, int* count, in
                                  int* threads_per_particle);
 /* Average device time (ms) of the list force kernel alone over reps launches, CUDA events on the batch stream. */
 md_status md_batch_time_forces(md_batch* b, int reps, double* ms);
+
+/* ---- trajectory adjoint --------------------------------------------------------------------------------
+ * Gradients of J = g_pe * mean_k U_k + g_pressure * mean_k P_k over an NVE velocity-Verlet trajectory of
+ * `steps` steps (k = 1..steps; P = (2 KE + W) / 3V, W the virial) with respect to epsilon, sigma and the
+ * initial positions and velocities. The reference has no adjoint; its step (src/Integrator.cpp:18-71), pair
+ * terms (src/Forcefield.cpp:25-36) and list rule (src/NeighbourList.cpp:11-134) define the trajectory, in FP64,
+ * with the particles kept in their input order. Checkpoints every checkpoint_every steps; the backward pass
+ * recomputes each segment from its checkpoint. forward/backward have torch.autograd.Function semantics: forward
+ * returns (mean U, mean P), backward takes their cotangents. */
+typedef struct md_adjoint md_adjoint;
+
+md_status md_adjoint_create(int device, int64_t n, double box_length, const double* pos4, const double* vel3,
+                            const double* mass, double epsilon, double sigma, double cutoff, double skin, double dt,
+                            int steps, int checkpoint_every, md_adjoint** out);
+md_status md_adjoint_destroy(md_adjoint* a);
+/* New epsilon and sigma, or a new initial state (pos4 / vel3 may be NULL to keep one); forward must follow. */
+md_status md_adjoint_set_parameters(md_adjoint* a, double epsilon, double sigma);
+md_status md_adjoint_set_state(md_adjoint* a, const double* pos4, const double* vel3);
+/* Runs the trajectory: mean U and mean P, and optionally U_k, W_k, KE_k for k = 1..steps (arrays of steps). */
+md_status md_adjoint_forward(md_adjoint* a, double* mean_pe, double* mean_pressure, double* pe_steps, double* w_steps,
+                             double* ke_steps);
+/* dJ/d epsilon, dJ/d sigma, dJ/d initial positions and velocities (3 x n component-major; NULL to skip) for the
+ * cotangents (g_pe, g_pressure) of the last forward's outputs. */
+md_status md_adjoint_backward(md_adjoint* a, double g_pe, double g_pressure, double* d_epsilon, double* d_sigma,
+                              double* d_pos3, double* d_vel3);
+/* Particles, steps, checkpoint interval, list builds of the last forward (the first included), kernels launched. */
+md_status md_adjoint_info(const md_adjoint* a, int64_t* n, int* steps, int* checkpoint_every, int* rebuilds,
+                          uint64_t* launches);
 
 #ifdef __cplusplus
 }

@@ -2,6 +2,7 @@
 // their device buffers and one CUDA stream per system; every kernel is in the md_*.cuh headers.
 #include "md_b200.h"
 
+#include "md_adjoint.cuh"
 #include "md_batch.cuh"
 #include "md_cells.cuh"
 #include "md_common.cuh"
@@ -466,12 +467,14 @@ md_status profile_collect(md_system* s) {
 // choice never changes a result. md_nlist_set_force_variant pins a variant instead.
 template <typename Launch>
 md_status choose_variant(md_system* s, md_nlist* nl, int prec, Launch&& launch) {
-    if (!nl->use_tiles) {
+    // variants available: 0 always, 1 with tiles, 2 (prefetching global gathers) for the float modes
+    unsigned mask = 1u | (nl->use_tiles ? 2u : 0u) | (prec == MD_PREC_FP32FX || prec == MD_PREC_FP32 ? 4u : 0u);
+    if (nl->variant[prec] >= 0 && ((mask >> nl->variant[prec]) & 1u)) return MD_OK;
+    if (mask == 1u) {
         nl->variant[prec] = 0;
         return MD_OK;
     }
-    if (nl->variant[prec] >= 0) return MD_OK;
-    if (nl->pinned[prec] >= 0) {
+    if (nl->pinned[prec] >= 0 && ((mask >> nl->pinned[prec]) & 1u)) {
         nl->variant[prec] = nl->pinned[prec];
         return MD_OK;
     }
@@ -479,8 +482,9 @@ md_status choose_variant(md_system* s, md_nlist* nl, int prec, Launch&& launch) 
     MD_CUDA(cudaEventCreate(&e0));
     MD_CUDA(cudaEventCreate(&e1));
     float best = 0.f;
-    int pick = 0;
-    for (int v = 0; v < 2; ++v) {
+    int pick = -1;
+    for (int v = 0; v < 3; ++v) {
+        if (!((mask >> v) & 1u)) continue;
         MD_TRY(launch(v));
         MD_CUDA(cudaEventRecord(e0, s->stream));
         MD_TRY(launch(v));
@@ -489,7 +493,7 @@ md_status choose_variant(md_system* s, md_nlist* nl, int prec, Launch&& launch) 
         MD_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
         MD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (v == 0 || ms < best) {
+        if (pick < 0 || ms < best) {
             best = ms;
             pick = v;
         }
@@ -1049,8 +1053,8 @@ md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_c
 }
 
 md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant) {
-    if (!nl || precision < MD_PREC_FP64 || precision > MD_PREC_FX64 || variant < -1 || variant > 1 ||
-        (precision == MD_PREC_FX64 && variant == 1))
+    if (!nl || precision < MD_PREC_FP64 || precision > MD_PREC_FX64 || variant < -1 || variant > 2 ||
+        (precision == MD_PREC_FX64 && variant >= 1) || (precision == MD_PREC_FP64 && variant == 2))
         return fail(MD_ERR_INVALID, "md_nlist_set_force_variant: bad arguments");
     nl->pinned[precision] = variant;
     nl->variant[precision] = -1;
@@ -1377,3 +1381,4 @@ extern "C" md_status md_kinetic_energy_noalloc(const double* vel3, const double*
 }
 
 #include "md_batch.inl"
+#include "md_adjoint.inl"

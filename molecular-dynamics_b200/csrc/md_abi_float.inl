@@ -126,14 +126,15 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
     if (n > 0) {
         const unsigned g = blocks_for(n, 128);
         if (nl->use_cells) {
-            // variant 0: global gathers (k_force_fp32_rows); variant 1: shared-memory tile (same bits)
+            // variant 0: global gathers (k_force_fp32_rows); 1: shared-memory tile; 2: global gathers with the rows
+            // prefetched a group ahead (all the same bits)
             if (!frames_fresh) MD_TRY(frames_async(s, nl));
             const TileGeom& tg = nl->tiles_geom;
             const CellOffsets offs = cell_offsets(nl, s);
             const size_t smem = sizeof(float4) * (tg.max_staged + 1);
             auto launch = [&](int variant, bool with_kick, bool energy) -> md_status {
                 const KickArgs ka{with_kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
-                auto go = [&](auto rows_kernel, auto tile_kernel) -> md_status {
+                auto go = [&](auto rows_kernel, auto tile_kernel, auto prefetch_kernel) -> md_status {
                     if (variant == 1) {
                         if (smem > kSmemNoOptIn)
                             MD_CUDA(cudaFuncSetAttribute(tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -141,6 +142,9 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
                         tile_kernel<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
                             nl->frames.p, s->pos.p, n, nl->grid.start.p, nl->cell_sorted.p, tg, lj, offs, nl->rows.p,
                             nl->cap, nl->counts.p, s->force.p, acc, ka);
+                    } else if (variant == 2) {
+                        prefetch_kernel<<<g, 128, 0, s->stream>>>(nl->frames.p, s->pos.p, n, s->box, lj, offs,
+                                                                  nl->rows.p, nl->cap, nl->counts.p, s->force.p, acc, ka);
                     } else {
                         rows_kernel<<<g, 128, 0, s->stream>>>(nl->frames.p, s->pos.p, n, s->box, lj, offs, nl->rows.p,
                                                               nl->cap, nl->counts.p, s->force.p, acc, ka);
@@ -149,10 +153,14 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
                     return MD_OK;
                 };
                 if (fixed)
-                    return energy ? go(k_force_fp32_rows<true, true>, k_force_fp32_tile<true, true>)
-                                  : go(k_force_fp32_rows<true, false>, k_force_fp32_tile<true, false>);
-                return energy ? go(k_force_fp32_rows<false, true>, k_force_fp32_tile<false, true>)
-                              : go(k_force_fp32_rows<false, false>, k_force_fp32_tile<false, false>);
+                    return energy ? go(k_force_fp32_rows<true, true>, k_force_fp32_tile<true, true>,
+                                       k_force_fp32_rows<true, true, true>)
+                                  : go(k_force_fp32_rows<true, false>, k_force_fp32_tile<true, false>,
+                                       k_force_fp32_rows<true, false, true>);
+                return energy ? go(k_force_fp32_rows<false, true>, k_force_fp32_tile<false, true>,
+                                   k_force_fp32_rows<false, true, true>)
+                              : go(k_force_fp32_rows<false, false>, k_force_fp32_tile<false, false>,
+                                   k_force_fp32_rows<false, false, true>);
             };
             MD_TRY(choose_variant(s, nl, ff->precision, [&](int v) { return launch(v, false, false); }));
             if (want_energy || kick) MD_CUDA(cudaMemsetAsync(ff->fx_acc.p, 0, 4 * sizeof(long long), s->stream));

@@ -26,6 +26,10 @@ __host__ __device__ __forceinline__ size_t row_index(int i, int s, int cap) {
 __device__ __forceinline__ uint4 row_quad(const uint32_t* __restrict__ rows, int i, int q, int cap) {
     return reinterpret_cast<const uint4*>(rows)[(static_cast<size_t>(i >> 5) * (cap >> 2) + q) * 32 + (i & 31)];
 }
+// row_quad with the streaming (evict-first) cache hint
+__device__ __forceinline__ uint4 row_quad_stream(const uint32_t* __restrict__ rows, int i, int q, int cap) {
+    return __ldcs(reinterpret_cast<const uint4*>(rows) + (static_cast<size_t>(i >> 5) * (cap >> 2) + q) * 32 + (i & 31));
+}
 inline size_t row_buffer_entries(long long n, int cap) { return static_cast<size_t>((n + 31) / 32) * 32 * cap; }
 
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
@@ -56,6 +60,11 @@ __device__ __forceinline__ double wrap(double x, const Box& b) {
 // dx^2 + dy^2 + dz^2 in the reference's left-to-right order
 __device__ __forceinline__ double norm2(double dx, double dy, double dz) {
     return dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+}
+
+// a1 b1 + a2 b2 + a3 b3 in left-to-right order
+__device__ __forceinline__ double norm2p(double a1, double b1, double a2, double b2, double a3, double b3) {
+    return dadd(dadd(dmul(a1, b1), dmul(a2, b2)), dmul(a3, b3));
 }
 
 // Lennard-Jones constants, precomputed on the host with the reference's expressions

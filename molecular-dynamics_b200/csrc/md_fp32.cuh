@@ -195,7 +195,10 @@ __global__ void k_frames(const double4* __restrict__ pos, int n, const int* __re
 
 // Thread per particle over its row with neighbour frames gathered from global memory (L1/L2); rows are read
 // as interleaved uint4, coalesced across the warp.
-template <bool kFixed, bool kEnergy>
+// kPrefetch (variant 2): row quads are loaded one group ahead with the streaming cache hint, so the next group's
+// entries are in flight while the current group's frames are gathered, and the streamed rows do not displace
+// the frames from L1/L2. Same arithmetic, same bits.
+template <bool kFixed, bool kEnergy, bool kPrefetch = false>
 __global__ void __launch_bounds__(128) k_force_fp32_rows(const float4* __restrict__ frames,
                                                          const double4* __restrict__ pos, int n, Box box,
                                                          FloatLJ lj, CellOffsets offs,
@@ -213,9 +216,24 @@ __global__ void __launch_bounds__(128) k_force_fp32_rows(const float4* __restric
         const int2 c = counts[i];
         const int groups = (c.x + c.y + 7) >> 3;  // rows are padded with sentinels to a multiple of 8
         FloatAcc<kFixed, kEnergy> a;
+        uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
+        if (kPrefetch && groups > 0) {
+            n0 = row_quad_stream(rows, i, 0, cap);
+            n1 = row_quad_stream(rows, i, 1, cap);
+        }
         for (int g = 0; g < groups; ++g) {
-            const uint4 e0 = row_quad(rows, i, 2 * g, cap);
-            const uint4 e1 = row_quad(rows, i, 2 * g + 1, cap);
+            uint4 e0, e1;
+            if (kPrefetch) {
+                e0 = n0;
+                e1 = n1;
+                if (g + 1 < groups) {
+                    n0 = row_quad_stream(rows, i, 2 * g + 2, cap);
+                    n1 = row_quad_stream(rows, i, 2 * g + 3, cap);
+                }
+            } else {
+                e0 = row_quad(rows, i, 2 * g, cap);
+                e1 = row_quad(rows, i, 2 * g + 1, cap);
+            }
             const uint32_t ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
             float gx = 0.f, gy = 0.f, gz = 0.f, ge = 0.f, gw = 0.f;
 #pragma unroll

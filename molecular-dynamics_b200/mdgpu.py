@@ -90,6 +90,12 @@ def _load():
         "md_batch_state_hash": (_I, [_P, _PU64]), "md_batch_rebuilds": (_I, [_P, _PU64]),
         "md_batch_set_force_variant": (_I, [_P, _I]), "md_batch_force_variant": (_I, [_P, _PI, _PI, _PI, _PI]),
         "md_batch_time_forces": (_I, [_P, _I, _PD]),
+        "md_adjoint_create": (_I, [_I, _I64, _D, _PD, _PD, _PD, _D, _D, _D, _D, _D, _I, _I, _PP]),
+        "md_adjoint_destroy": (_I, [_P]), "md_adjoint_set_parameters": (_I, [_P, _D, _D]),
+        "md_adjoint_set_state": (_I, [_P, _PD, _PD]),
+        "md_adjoint_forward": (_I, [_P, _PD, _PD, _PD, _PD, _PD]),
+        "md_adjoint_backward": (_I, [_P, _D, _D, _PD, _PD, _PD, _PD]),
+        "md_adjoint_info": (_I, [_P, C.POINTER(C.c_int64), _PI, _PI, _PI, _PU64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -606,4 +612,80 @@ class Batch:
         p = C.c_void_p()
         _check(LIB.md_batch_stream(self.h, C.byref(p)))
         return p.value or 0
+
+
+class Adjoint:
+    """Trajectory adjoint (md_adjoint_*): J = g_pe * mean U + g_pressure * mean P over `steps` NVE steps of the
+    system (pos (n, 4), box, vel (3, n), mass (n,) or None), differentiated with respect to epsilon, sigma and
+    the initial positions and velocities. forward() -> (mean U, mean P); backward(g_pe, g_pressure) -> dict of
+    gradients (d_pos and d_vel as (3, n) component arrays, like the velocities)."""
+
+    def __init__(self, pos, box, vel, mass=None, epsilon=1.0, sigma=1.0, cutoff=2.5, skin=0.3, dt=0.005, steps=200,
+                 checkpoint_every=20, device=0):
+        p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 4)
+        v = np.ascontiguousarray(vel, dtype=np.float64).reshape(3, -1)
+        m = None if mass is None else np.ascontiguousarray(mass, dtype=np.float64)
+        self.n, self.box, self.steps = len(p), float(box), steps
+        h = C.c_void_p()
+        _check(LIB.md_adjoint_create(device, self.n, self.box, _pd(p), _pd(v), _pd(m), epsilon, sigma, cutoff, skin,
+                                     dt, steps, checkpoint_every, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            LIB.md_adjoint_destroy(self.h)
+            self.h = None
+
+    def set_parameters(self, epsilon: float, sigma: float):
+        _check(LIB.md_adjoint_set_parameters(self.h, float(epsilon), float(sigma)))
+
+    def set_state(self, pos=None, vel=None):
+        p = None if pos is None else np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 4)
+        v = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64).reshape(3, -1)
+        _check(LIB.md_adjoint_set_state(self.h, _pd(p), _pd(v)))
+
+    def forward(self, record: bool = False):
+        mu, mp = C.c_double(), C.c_double()
+        if not record:
+            _check(LIB.md_adjoint_forward(self.h, C.byref(mu), C.byref(mp), None, None, None))
+            return mu.value, mp.value
+        u, w, k = np.zeros(self.steps), np.zeros(self.steps), np.zeros(self.steps)
+        _check(LIB.md_adjoint_forward(self.h, C.byref(mu), C.byref(mp), _pd(u), _pd(w), _pd(k)))
+        return mu.value, mp.value, u, w, k
+
+    def backward(self, g_pe: float, g_pressure: float) -> dict:
+        de, ds = C.c_double(), C.c_double()
+        dp, dv = np.zeros((3, self.n)), np.zeros((3, self.n))
+        _check(LIB.md_adjoint_backward(self.h, float(g_pe), float(g_pressure), C.byref(de), C.byref(ds), _pd(dp),
+                                       _pd(dv)))
+        return dict(d_epsilon=de.value, d_sigma=ds.value, d_pos=dp, d_vel=dv)
+
+    def info(self) -> dict:
+        n, st, ev, rb, la = C.c_int64(), C.c_int(), C.c_int(), C.c_int(), C.c_uint64()
+        _check(LIB.md_adjoint_info(self.h, C.byref(n), C.byref(st), C.byref(ev), C.byref(rb), C.byref(la)))
+        return dict(n=n.value, steps=st.value, checkpoint_every=ev.value, rebuilds=rb.value, launches=la.value)
+
+
+def trajectory_observables(epsilon, sigma, pos, engine: Adjoint):
+    """torch.autograd.Function over an Adjoint engine: (epsilon, sigma, pos (n, 3)) tensors in float64 ->
+    tensor([mean U, mean P]); backward returns the engine's gradients. The initial velocities are the engine's."""
+    import torch
+
+    class _TrajectoryObservables(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, eps, sig, p):
+            engine.set_parameters(float(eps), float(sig))
+            p4 = np.zeros((engine.n, 4))
+            p4[:, :3] = p.detach().cpu().numpy()
+            engine.set_state(pos=p4)
+            u, pr = engine.forward()
+            return torch.tensor([u, pr], dtype=torch.float64)
+
+        @staticmethod
+        def backward(ctx, g):
+            r = engine.backward(float(g[0]), float(g[1]))
+            return (torch.tensor(r["d_epsilon"], dtype=torch.float64), torch.tensor(r["d_sigma"], dtype=torch.float64),
+                    torch.from_numpy(np.ascontiguousarray(r["d_pos"].T)))
+
+    return _TrajectoryObservables.apply(epsilon, sigma, pos)
 

@@ -151,6 +151,11 @@ class Oracle(_Lib):
         L.orc_step.argtypes = [_P, _P, _P, _D, _I, _PD]
         L.orc_rdf_sample.argtypes = [_P, _P, _D, _I, _PD]
         L.orc_rdf_values.argtypes = [_PD, _I, _D, _I, _D, _D, _PD]
+        L.orc_adj_create.restype = _P
+        L.orc_adj_create.argtypes = [_I64, _D, _PD, _PD, _PD, _D, _D, _D, _D, _D, _I, _I]
+        L.orc_adj_destroy.argtypes = [_P]
+        L.orc_adj_forward.argtypes = [_P, _PD, _PD, _PD, _PD, _PD]
+        L.orc_adj_backward.argtypes = [_P, _D, _D, _PD, _PD, _PD, _PD]
 
     def error(self) -> str:
         return self.lib.orc_last_error().decode()
@@ -343,6 +348,39 @@ def rdf_sample(o: Oracle, s: OSystem, nl: ONeighbourList, rmax: float, bins: int
     o.lib.orc_rdf_sample(s.h, nl.h, rmax, bins, _pd(hist))
 
 
+class OAdjoint:
+    """The FP64 CPU adjoint of the trajectory (md_adjoint.cpp): J = g_pe mean U + g_p mean P over `steps` steps."""
+
+    def __init__(self, o: Oracle, pos, box, vel, mass=None, eps=1.0, sigma=1.0, rc=2.5, skin=0.3, dt=0.005,
+                 steps=200, every=20):
+        self.o = o
+        self.n = len(pos)
+        self.steps = steps
+        p = np.ascontiguousarray(pos, dtype=np.float64)
+        v = np.ascontiguousarray(vel, dtype=np.float64)
+        m = None if mass is None else np.ascontiguousarray(mass, dtype=np.float64)
+        self.h = o.lib.orc_adj_create(self.n, box, _pd(p), _pd(v), _pd(m), eps, sigma, rc, skin, dt, steps, every)
+
+    def __del__(self):
+        try:
+            self.o.lib.orc_adj_destroy(self.h)
+        except Exception:
+            pass
+
+    def forward(self):
+        """(mean U, mean P, U_k, W_k, KE_k)"""
+        mu, mp = C.c_double(), C.c_double()
+        u, w, k = np.zeros(self.steps), np.zeros(self.steps), np.zeros(self.steps)
+        self.o.lib.orc_adj_forward(self.h, C.byref(mu), C.byref(mp), _pd(u), _pd(w), _pd(k))
+        return mu.value, mp.value, u, w, k
+
+    def backward(self, g_pe, g_p):
+        de, ds = C.c_double(), C.c_double()
+        dp, dv = np.zeros((3, self.n)), np.zeros((3, self.n))
+        self.o.lib.orc_adj_backward(self.h, g_pe, g_p, C.byref(de), C.byref(ds), _pd(dp), _pd(dv))
+        return dict(d_epsilon=de.value, d_sigma=ds.value, d_pos=dp, d_vel=dv)
+
+
 class Reference(_Lib):
     """The reference's own classes (oracle/_ref/libmdref.so, built from its unmodified sources)."""
 
@@ -398,6 +436,8 @@ class Reference(_Lib):
         L.ref_ff_forces_all.argtypes = [_P, _P, _PD]
         L.ref_run.restype = _I
         L.ref_run.argtypes = [_P, _P, _P, _D, _I, _I, _D, _PD, _PD]
+        L.ref_run_observables.restype = _I
+        L.ref_run_observables.argtypes = [_P, _P, _P, _D, _I, _PD, _PD, _PD]
         L.ref_bussi_create.restype = _P
         L.ref_bussi_create.argtypes = [_D, _D, _U64]
         L.ref_bussi_destroy.argtypes = [_P]
@@ -561,6 +601,13 @@ class RForceField:
                               _pd(pe), _pd(ke)) != 0:
             raise RuntimeError(self.r.error())
         return pe, ke
+
+    def observables(self, s: RSystem, nl: RNeighbourList, dt: float, steps: int):
+        """`steps` NVE steps through the reference's integrator: per-step (PE, virial, KE)."""
+        pe, w, ke = np.zeros(steps), np.zeros(steps), np.zeros(steps)
+        if self.r.lib.ref_run_observables(s.h, self.h, nl.h, dt, steps, _pd(pe), _pd(w), _pd(ke)) != 0:
+            raise RuntimeError(self.r.error())
+        return pe, w, ke
 
     @property
     def shift(self):

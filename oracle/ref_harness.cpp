@@ -177,6 +177,19 @@ int ref_run(System* s, LennardJonesForceField* f, NeighbourList* nl, double dt, 
     });
 }
 
+// NVE steps recording the potential energy, the virial (getVirial) and the kinetic energy after each step
+int ref_run_observables(System* s, LennardJonesForceField* f, NeighbourList* nl, double dt, int n_steps, double* pe,
+                        double* w, double* ke) {
+    return guarded([&] {
+        VelocityVerletIntegrator integ(dt);
+        for (int k = 0; k < n_steps; ++k) {
+            pe[k] = integ.step(*s, *f, *nl);
+            w[k] = f->getVirial();
+            ke[k] = s->kineticEnergy();
+        }
+    });
+}
+
 BussiThermostat* ref_bussi_create(double t, double tau, std::uint64_t seed) { return new BussiThermostat(t, tau, seed); }
 void ref_bussi_destroy(BussiThermostat* b) { delete b; }
 void ref_bussi_apply(BussiThermostat* b, System* s, double dt) { b->apply(*s, dt); }

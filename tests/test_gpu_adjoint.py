@@ -1,0 +1,90 @@
+"""The GPU trajectory adjoint (md_adjoint_*) against the FP64 CPU adjoint (oracle/md_adjoint.cpp) bit for bit,
+against central finite differences of its own forward pass, and through its torch.autograd.Function.
+
+Differentiation workload: N = 32,000 (FCC 20^3 x 4), density 0.8442, T* = 1.0, 200 NVE steps of dt = 0.005,
+checkpoints every 20 steps; gradients of the time averages of the potential energy and the virial pressure with
+respect to epsilon, sigma and the initial positions (and velocities)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle.oracle import OAdjoint
+
+pytestmark = pytest.mark.gpu
+
+
+def engines(md, oracle, cells, density, temperature, steps, every):
+    s = oracle.fcc_system(cells, density, temperature, 42)
+    st = s.state()
+    gpu = md.Adjoint(st.pos, st.box, st.vel, steps=steps, checkpoint_every=every)
+    cpu = OAdjoint(oracle, st.pos, st.box, st.vel, steps=steps, every=every)
+    return st, gpu, cpu
+
+
+@pytest.mark.parametrize("cells,density,temperature,steps,every",
+                         [(4, 0.8442, 1.0, 60, 20), (6, 0.75, 1.5, 70, 25), (20, 0.8442, 1.0, 200, 20)])
+def test_gpu_adjoint_bit_identical_to_cpu_adjoint(md, oracle, cells, density, temperature, steps, every):
+    st, gpu, cpu = engines(md, oracle, cells, density, temperature, steps, every)
+    mu, mp, u, w, k = gpu.forward(record=True)
+    cu, cp, ou, ow, ok = cpu.forward()
+    assert (mu, mp) == (cu, cp)
+    assert np.array_equal(u, ou) and np.array_equal(w, ow) and np.array_equal(k, ok)
+    for g_pe, g_p in ((1.0, 0.0), (0.0, 1.0), (0.3, -1.7)):
+        a = gpu.backward(g_pe, g_p)
+        b = cpu.backward(g_pe, g_p)
+        assert a["d_epsilon"] == b["d_epsilon"] and a["d_sigma"] == b["d_sigma"], (g_pe, g_p)
+        assert np.array_equal(a["d_pos"], b["d_pos"]) and np.array_equal(a["d_vel"], b["d_vel"]), (g_pe, g_p)
+    assert gpu.info()["rebuilds"] >= 1
+
+
+def central(f, h):
+    return (f(h) - f(-h)) / (2 * h)
+
+
+def test_gpu_adjoint_against_central_differences(md, oracle):
+    """The differentiation workload. The truncated force jumps at r_c, so a stencil that moves a pair across the
+    cutoff at some step adds a jump the derivative does not have: h = 1e-4 shows this at the 1e-5..1e-2 level;
+    the derivative itself is checked at the smaller h where the stencil is clean (relative error < 1e-6)."""
+    st, gpu, _ = engines(md, oracle, 20, 0.8442, 1.0, 200, 20)
+    rng = np.random.default_rng(3)
+    dp = np.zeros_like(st.pos)
+    dp[:, :3] = rng.standard_normal((len(st.pos), 3))
+    dp /= np.linalg.norm(dp)
+    for g_pe, g_p in ((1.0, 0.0), (0.0, 1.0)):
+        gpu.set_parameters(1.0, 1.0)
+        gpu.set_state(pos=st.pos)
+        gpu.forward()
+        g = gpu.backward(g_pe, g_p)
+
+        def J(eps=1.0, sig=1.0, pos=st.pos):
+            gpu.set_parameters(eps, sig)
+            gpu.set_state(pos=pos)
+            u, p = gpu.forward()
+            return g_pe * u + g_p * p
+
+        checks = {"epsilon": (g["d_epsilon"], lambda h: J(eps=1.0 + h)),
+                  "sigma": (g["d_sigma"], lambda h: J(sig=1.0 + h)),
+                  "positions": (float((g["d_pos"].T * dp[:, :3]).sum()), lambda h: J(pos=st.pos + h * dp))}
+        for name, (adj, f) in checks.items():
+            errs = {h: abs(central(f, h) - adj) / abs(adj) for h in (1e-4, 1e-6, 1e-7, 1e-8)}
+            print(name, g_pe, g_p, adj, errs)
+            assert min(errs.values()) < 1e-6, (name, adj, errs)
+    gpu.set_parameters(1.0, 1.0)
+    gpu.set_state(pos=st.pos)
+
+
+def test_autograd_function(md, oracle):
+    import torch
+
+    st, gpu, _ = engines(md, oracle, 6, 0.8442, 1.0, 40, 20)
+    eps = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    sig = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    pos = torch.tensor(st.pos[:, :3], dtype=torch.float64, requires_grad=True)
+    out = md.trajectory_observables(eps, sig, pos, gpu)
+    (out[0] * 0.5 + out[1] * 2.0).backward()
+    ref = gpu.backward(0.5, 2.0)
+    assert eps.grad.item() == ref["d_epsilon"] and sig.grad.item() == ref["d_sigma"]
+    assert np.array_equal(pos.grad.numpy(), ref["d_pos"].T)
+    mu, mp = gpu.forward()
+    assert out[0].item() == mu and out[1].item() == mp

@@ -396,8 +396,9 @@ def test_larger_systems_match_oracle(md, oracle, cells, density):
 
 @pytest.mark.parametrize("cells,density", [(8, 0.8442), (40, 0.8442), (40, 1.0)])
 def test_force_kernel_variants_agree_bit_for_bit(md, cells, density):
-    """The autotuner may pick the global-gather or the shared-memory tile force kernel; both (and the fused
-    kick) give the same bits in every precision, so the choice never changes a trajectory."""
+    """The autotuner may pick the global-gather, the shared-memory tile or the prefetching global-gather force
+    kernel; all (and the fused kick) give the same bits in every precision, so the choice never changes a
+    trajectory."""
     import numpy as np
 
     base = md.fcc_system(cells, density, 1.2, seed=7)
@@ -407,17 +408,18 @@ def test_force_kernel_variants_agree_bit_for_bit(md, cells, density):
     st = base.download()
     for prec in (md.PREC_FP64, md.PREC_FP32FX, md.PREC_FP32):
         results = []
-        for variant in (0, 1):
+        for variant in ((0, 1) if prec == md.PREC_FP64 else (0, 1, 2)):
             s = md.System.from_arrays(st["pos"], base.box, vel=st["vel"], force=st["force"])
             nl = md.NeighbourList(2.5, 0.3)
             nl.set_force_variant(prec, variant)
             nl.build(s)
             ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)
             pe, ke, w = md.VelocityVerletIntegrator(0.005).run(s, ff, nl, 20)
-            if nl.layout()["use_tiles"]:
+            if nl.layout()["use_tiles"] or variant != 1:
                 assert nl.force_variant(prec) == variant
             results.append((pe, ke, w, s.download()))
-        (pa, ka, wa, sa), (pb, kb, wb, sb) = results
-        assert np.array_equal(pa, pb) and np.array_equal(ka, kb) and np.array_equal(wa, wb), prec
-        for k in ("pos", "vel", "force"):
-            assert np.array_equal(sa[k], sb[k]), (prec, k)
+        pa, ka, wa, sa = results[0]
+        for pb, kb, wb, sb in results[1:]:
+            assert np.array_equal(pa, pb) and np.array_equal(ka, kb) and np.array_equal(wa, wb), prec
+            for k in ("pos", "vel", "force"):
+                assert np.array_equal(sa[k], sb[k]), (prec, k)
