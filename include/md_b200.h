@@ -108,6 +108,14 @@ md_status md_initialize_velocities(md_system* s, double temperature, uint32_t se
  * current device must be the one holding the pointers. No allocating call is made. */
 md_status md_kinetic_energy_noalloc(const double* vel3, const double* mass, int64_t n, double* out, void* stream);
 
+/* writeXyzFrame's data (src/Trajectory.cpp:4-25) in id order: out6[6 id + k] = (x, y, z, vx, vy, vz)[k] of
+ * the particle with that id, gathered through the ids on the device and copied to the host in one transfer on a
+ * second stream. With wait = 0 the call returns once the copy is queued (out6 should then be pinned memory) and
+ * the system's stream may keep stepping; md_system_frame_wait blocks until the copy has landed. A new frame
+ * waits for the previous one's copy. */
+md_status md_system_frame_by_id(md_system* s, double* out6, int wait);
+md_status md_system_frame_wait(md_system* s);
+
 /* ---- streams, timing and counters ---------------------------------------------------------------------- */
 /* The cudaStream_t every call on this system is queued on (for CUDA events around calls). */
 md_status md_system_stream(md_system* s, void** stream);

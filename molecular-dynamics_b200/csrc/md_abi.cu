@@ -116,6 +116,10 @@ struct md_system {
     size_t events_used = 0;
     double profile_ms = 0.0;
     int64_t profile_count = 0;
+    // md_system_frame_by_id: id-ordered staging buffer, its copy stream and the event that orders them
+    DevBuf<double> frame;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t frame_ready = nullptr;
 };
 
 struct CellGrid {
@@ -698,10 +702,43 @@ md_status md_system_destroy(md_system* s) {
     if (g_launches == &s->launches) g_launches = nullptr;
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
     for (cudaEvent_t e : s->events) cudaEventDestroy(e);
+    if (s->frame_ready) cudaEventDestroy(s->frame_ready);
     if (s->host_scal) cudaFreeHost(s->host_scal);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
+    return MD_OK;
+}
+
+// Trajectory.cpp:4-25's frame in id order: a device scatter through the ids (the inverse of the list's
+// permutation) into a staging buffer, then one copy to the host on a second stream, so the system's stream
+// can go on stepping while the frame travels and the host formats the previous one.
+md_status md_system_frame_by_id(md_system* s, double* out6, int wait) {
+    if (!s || !out6) return fail(MD_ERR_INVALID, "md_system_frame_by_id: bad arguments");
+    MD_TRY(use_system(s));
+    const int n = static_cast<int>(s->n);
+    if (!s->copy_stream) MD_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+    if (!s->frame_ready) MD_CUDA(cudaEventCreateWithFlags(&s->frame_ready, cudaEventDisableTiming));
+    // the previous frame's copy must be done with the staging buffer
+    MD_CUDA(cudaStreamSynchronize(s->copy_stream));
+    MD_CUDA(s->frame.reserve(6 * static_cast<size_t>(n)));
+    if (n > 0) {
+        k_frame_by_id<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(s->pos.p, s->vel.p, s->ids.p, n, s->frame.p);
+        MD_CHECK_LAUNCH();
+    }
+    MD_CUDA(cudaEventRecord(s->frame_ready, s->stream));
+    MD_CUDA(cudaStreamWaitEvent(s->copy_stream, s->frame_ready, 0));
+    MD_CUDA(cudaMemcpyAsync(out6, s->frame.p, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s->copy_stream));
+    if (wait) MD_CUDA(cudaStreamSynchronize(s->copy_stream));
+    return MD_OK;
+}
+
+md_status md_system_frame_wait(md_system* s) {
+    if (!s) return fail(MD_ERR_INVALID, "null system");
+    MD_TRY(use_system(s));
+    if (s->copy_stream) MD_CUDA(cudaStreamSynchronize(s->copy_stream));
     return MD_OK;
 }
 

@@ -102,4 +102,22 @@ __global__ void k_permute_commit(int n, const uint32_t* __restrict__ order, cons
     if (ref_pos) ref_pos[k] = p;
 }
 
+// out[6 id + k] = (x, y, z, vx, vy, vz)[k] of the particle whose id is `id` (ids are a permutation of 0..n-1;
+// an id out of range is skipped)
+__global__ void k_frame_by_id(const double4* __restrict__ pos, const double* __restrict__ vel,
+                              const uint64_t* __restrict__ ids, int n, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t id = ids[i];
+    if (id >= static_cast<uint64_t>(n)) return;
+    double* o = out + 6 * id;
+    const double4 p = pos[i];
+    o[0] = p.x;
+    o[1] = p.y;
+    o[2] = p.z;
+    o[3] = vel[i];
+    o[4] = vel[static_cast<size_t>(n) + i];
+    o[5] = vel[2 * static_cast<size_t>(n) + i];
+}
+
 }  // namespace md

@@ -451,19 +451,16 @@ void initializeVelocities(System& system, double temperature, std::uint32_t seed
 void writeXyzFrame(std::FILE* file, const System& system, double time) {
     const std::size_t n = system.size();
     const double l = system.getBoxLength();
-    const auto ids = system.ids();
-    std::vector<std::size_t> where(n);  // storage index of each id
-    for (std::size_t i = 0; i < n; ++i) where[ids[i]] = i;
+    // the frame in id order, gathered on the device (md_system_frame_by_id)
+    std::vector<double> f(6 * n);
+    check(md_system_frame_by_id(system.handle(), f.data(), 1));
     std::fprintf(file, "%zu\n", n);
     std::fprintf(file,
                  "Lattice=\"%.10g 0 0 0 %.10g 0 0 0 %.10g\" Properties=species:S:1:pos:R:3:velo:R:3:id:I:1 "
                  "Time=%.6f pbc=\"T T T\"\n",
                  l, l, l, time);
-    const double* r = system.packedPositions();
-    const auto vx = system.velocity(0), vy = system.velocity(1), vz = system.velocity(2);
     for (std::size_t id = 0; id < n; ++id) {
-        const std::size_t i = where[id];
-        std::fprintf(file, "Ar %.8f %.8f %.8f %.8f %.8f %.8f %zu\n", r[4 * i], r[4 * i + 1], r[4 * i + 2], vx[i], vy[i],
-                     vz[i], id);
+        const double* r = f.data() + 6 * id;
+        std::fprintf(file, "Ar %.8f %.8f %.8f %.8f %.8f %.8f %zu\n", r[0], r[1], r[2], r[3], r[4], r[5], id);
     }
 }

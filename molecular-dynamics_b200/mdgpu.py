@@ -81,6 +81,7 @@ def _load():
         "md_system_launch_count": (_I, [_P, _PU64]), "md_profile_enable": (_I, [_P, _I]),
         "md_profile_read": (_I, [_P, _PD, C.POINTER(C.c_int64)]),
         "md_forcefield_results": (_I, [_P, _PD, _PD]),
+        "md_system_frame_by_id": (_I, [_P, _PD, _I]), "md_system_frame_wait": (_I, [_P]),
         "md_batch_create": (_I, [_I, _I, C.POINTER(C.c_int64), _PD, _PD, _PU64, _PD, _PD, _PD,
                                  C.POINTER(md_batch_options), _PP]),
         "md_batch_destroy": (_I, [_P]), "md_batch_info": (_I, [_P, _PI, C.POINTER(C.c_int64), _PI, _PU64]),
@@ -194,6 +195,12 @@ class System:
         pos, vel, force, mass = f64(pos, (self.n, 4)), f64(vel, (3, self.n)), f64(force, (3, self.n)), f64(mass, (self.n,))
         ids = None if ids is None else np.ascontiguousarray(ids, dtype=np.uint64)
         _check(LIB.md_system_upload(self.h, _pd(pos), _pd(vel), _pd(force), _pd(mass), _pu(ids)))
+
+    def frame_by_id(self) -> np.ndarray:
+        """(n, 6) array of (x, y, z, vx, vy, vz) in id order, gathered on the device (writeXyzFrame's data)."""
+        out = np.zeros((self.n, 6))
+        _check(LIB.md_system_frame_by_id(self.h, _pd(out), 1))
+        return out
 
     def download(self):
         pos = np.zeros((self.n, 4))

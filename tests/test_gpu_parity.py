@@ -423,3 +423,22 @@ def test_force_kernel_variants_agree_bit_for_bit(md, cells, density):
             assert np.array_equal(pa, pb) and np.array_equal(ka, kb) and np.array_equal(wa, wb), prec
             for k in ("pos", "vel", "force"):
                 assert np.array_equal(sa[k], sb[k]), (prec, k)
+
+
+def test_frame_by_id_inverts_the_list_permutation(md):
+    """md_system_frame_by_id (writeXyzFrame's data, src/Trajectory.cpp:4-25): after rebuilds have reordered
+    the particles, the device gather through the ids equals the host-side inverse permutation."""
+    s = md.fcc_system(8, 0.8442, 1.5, seed=3)
+    nl = md.NeighbourList(2.5, 0.3)
+    nl.build(s)
+    ff = md.LennardJonesForceField(1.0, 1.0, 2.5)
+    ff.compute_forces(s, nl)
+    md.VelocityVerletIntegrator(0.005).run(s, ff, nl, 100, record=False)
+    assert nl.rebuild_count > 1
+    st = s.download()
+    frame = s.frame_by_id()
+    where = np.empty(s.n, dtype=np.int64)
+    where[st["ids"].astype(np.int64)] = np.arange(s.n)
+    assert np.array_equal(frame[:, :3], st["pos"][where, :3])
+    assert np.array_equal(frame[:, 3:], st["vel"][:, where].T)
+    assert np.array_equal(s.frame_by_id(), frame)
