@@ -61,6 +61,11 @@ def args_parse():
     p.add_argument("--sweep", choices=["precision"], default=None,
                    help="instead of the headline line: the N=256,000 precision sweep over densities {0.5, 0.8442, 1.0} "
                         "x T {0.71, 1.5, 3.0} (one JSON line per state point; --steps NVE steps each)")
+    p.add_argument("--replica-steps", type=int, default=5000,
+                   help="steps of the batched-replica workload (512 replicas; 0: skip)")
+    p.add_argument("--replicas", type=int, default=512)
+    p.add_argument("--adjoint-steps", type=int, default=200,
+                   help="trajectory length of the differentiation workload (N = 32,000; 0: skip)")
     p.add_argument("--profile-region", action="store_true",
                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return p.parse_args()
@@ -262,6 +267,103 @@ def force_errors(md, s, nl) -> dict:
     return out
 
 
+def block_error(x, blocks: int = 10):
+    """Mean and its standard error from `blocks` block averages of the rows of x (samples x replicas)."""
+    import numpy as np
+
+    m = (x.shape[0] // blocks) * blocks
+    b = x[:m].reshape(blocks, m // blocks, *x.shape[1:]).mean(axis=1)
+    return b.mean(axis=0), b.std(axis=0, ddof=1) / np.sqrt(blocks)
+
+
+def replica_workload(md, a, device: int) -> dict:
+    """The batched-replica workload: `a.replicas` independent LJ systems, N = 4 n^3 with n uniform in [4, 20],
+    density uniform in [0.7, 0.95], T* uniform in [0.7, 2.0] (all drawn from one generator with a fixed seed),
+    seeded FCC starts, Bussi NVT with tau = 0.1, dt = 0.005, r_c = 2.5, skin 0.3, in one md_batch (CUDA graphs of
+    100 steps, per-replica device-side rebuilds). Aggregate atom-steps/s over `a.replica_steps` steps after 100
+    untimed ones, and per-replica means with block-averaged error bars of PE/N and the virial pressure."""
+    import numpy as np
+    import torch
+
+    rng = np.random.default_rng(20240611)
+    R = a.replicas
+    cells = rng.integers(4, 21, size=R)
+    rho = rng.uniform(0.7, 0.95, size=R)
+    temp = rng.uniform(0.7, 2.0, size=R)
+    systems = []
+    for k in range(R):
+        s = md.fcc_system(int(cells[k]), float(rho[k]), float(temp[k]), seed=1000 + k, device=device)
+        d = s.download()
+        systems.append((d["pos"], s.box, d["vel"], None))
+        del s
+    prec = PRECISIONS[a.precision][0]
+    b = md.Batch(systems, precision=prec, thermostat="bussi", temperatures=temp, seeds=1000 + np.arange(R),
+                 bussi_tau=0.1, energy_every=10, chunk_steps=100, device=device)
+    info = b.info()
+    b.run(100)
+    stream = torch.cuda.ExternalStream(b.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    l0 = b.info()["launches"]
+    e0.record(stream)
+    pe, w, ke = b.run(a.replica_steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    n = np.array([len(p) for p, *_ in systems], dtype=np.float64)
+    vol = np.array([bx ** 3 for _, bx, *_ in systems])
+    keep = pe.shape[0] // 5  # the first fifth of the samples is equilibration
+    pe_n, pe_err = block_error(pe[keep:] / n)
+    p_mean, p_err = block_error((2 * ke[keep:] + w[keep:]) / (3 * vol))
+    t_mean = (2 * ke[keep:] / (3 * n - 3)).mean(axis=0)
+    return {"workload": f"{R} replicas, n~U[4,20] (N 256-32000), rho~U[0.7,0.95], T~U[0.7,2.0], Bussi tau=0.1, "
+                        f"dt=0.005, rc=2.5, skin=0.3, {a.replica_steps} steps",
+            "atoms": info["atoms"], "value": info["atoms"] * a.replica_steps / (ms / 1e3), "unit": "atom-steps/s",
+            "ms_per_step": ms / a.replica_steps, "precision": a.precision,
+            "force_variant": b.force_variant(), "gpu_launches": b.info()["launches"] - l0,
+            "rebuilds_per_replica_mean": float(b.rebuilds().mean()),
+            "pe_per_atom_stderr": {"median": float(np.median(pe_err)), "max": float(pe_err.max())},
+            "pressure_stderr": {"median": float(np.median(p_err)), "max": float(p_err.max())},
+            "mean_T_rel_dev_from_target": {"median": float(np.median(np.abs(t_mean / temp - 1))),
+                                           "max": float(np.abs(t_mean / temp - 1).max())},
+            "examples": [{"n": int(n[k]), "rho": float(rho[k]), "T": float(temp[k]),
+                          "pe_per_atom": [float(pe_n[k]), float(pe_err[k])], "pressure": [float(p_mean[k]), float(p_err[k])]}
+                         for k in range(3)]}
+
+
+def adjoint_workload(md, a, device: int) -> dict:
+    """The differentiation workload: N = 32,000 (FCC 20^3 x 4), density 0.8442, T* = 1.0, `a.adjoint_steps` NVE
+    steps of dt = 0.005, checkpoints every 20; timings of forward and backward, and the gradient of mean U with
+    respect to epsilon against central differences at h = 1e-4 (the cutoff's force jump enters the stencil),
+    1e-7 and 1e-8."""
+    import torch
+
+    s = md.fcc_system(20, 0.8442, 1.0, seed=42, device=device)
+    d = s.download()
+    eng = md.Adjoint(d["pos"], s.box, d["vel"], steps=a.adjoint_steps, checkpoint_every=20, device=device)
+    eng.forward()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mu, mp = eng.forward()
+    t1 = time.perf_counter()
+    g = eng.backward(1.0, 0.0)
+    t2 = time.perf_counter()
+
+    def J(eps):
+        eng.set_parameters(eps, 1.0)
+        return eng.forward()[0]
+
+    fd = {h: (J(1.0 + h) - J(1.0 - h)) / (2 * h) for h in (1e-4, 1e-7, 1e-8)}
+    eng.set_parameters(1.0, 1.0)
+    n = s.n
+    return {"workload": f"N={n} FCC 20^3x4, rho=0.8442, T=1.0, {a.adjoint_steps} NVE steps, checkpoints every 20",
+            "mean_pe": mu, "mean_pressure": mp, "forward_s": t1 - t0, "backward_s": t2 - t1,
+            "forward_atom_steps_per_s": n * a.adjoint_steps / (t1 - t0),
+            "d_mean_pe_d_epsilon": g["d_epsilon"], "d_mean_pe_d_sigma": g["d_sigma"],
+            "fd_rel_err_epsilon": {str(h): abs(v - g["d_epsilon"]) / abs(g["d_epsilon"]) for h, v in fd.items()},
+            "rebuilds": eng.info()["rebuilds"]}
+
+
 def run_gpu_arm(a):
     import numpy as np
     import torch
@@ -316,6 +418,7 @@ def run_gpu_arm(a):
     force_ms, force_n = s.profile_read()
     s.profile(False)
     launches = s.launch_count - l0
+    variant = nl.force_variant(prec)
     rebuilds = nl.rebuild_count - rb0
     pairs = nl.pair_count
     if dist:
@@ -397,6 +500,9 @@ def run_gpu_arm(a):
                            "per-step PE/KE/virial read back, D2H of final positions/velocities"}
         del s2, nl2, ff2
 
+    replicas = replica_workload(md, a, local) if rank == 0 and a.replica_steps > 0 else None
+    adjoint = adjoint_workload(md, a, local) if rank == 0 and a.adjoint_steps > 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and a.cpu_steps > 0:
         cb = reference_sample(a, a.cpu_steps, 1)
@@ -419,13 +525,15 @@ def run_gpu_arm(a):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None if tpa is None else tpa * n,
                          "kernel": {"fp64": "k_force_fp64", "fx64": "k_force_fx64_rows"}.get(a.precision, "k_force_fp32"),
+                         "force_variant": {0: "global gathers", 1: "shared-memory tiles",
+                                           2: "global gathers, rows prefetched"}.get(variant, str(variant)),
                          "kernel_ms": kernel_s * 1e3,
                          "algorithmic_bytes_per_atom": bytes_per_atom, "peak_source": peak_src},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
             "rebuilds": rebuilds, "half_list_pairs": pairs, "max_energy_drift": drift,
             "fp64": fp64, "speedup_vs_fp64": None if fp64 is None else value / world / fp64["value"],
             "other_precisions": others,
-            "force_error_vs_fp64": errors}
+            "force_error_vs_fp64": errors, "replicas": replicas, "adjoint": adjoint}
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
