@@ -44,15 +44,17 @@ def central(f, h):
 
 @pytest.mark.parametrize("cells,steps,params,hs", [
     (6, 100, ("epsilon", "sigma", "positions"), (1e-5, 1e-6, 1e-7)),
-    (20, 200, ("epsilon", "positions"), (1e-6, 1e-7, 1e-8)),
+    (20, 200, ("epsilon",), (1e-7, 1e-8)),
 ])
 def test_gpu_adjoint_against_central_differences(md, oracle, cells, steps, params, hs):
     """Central differences of the GPU forward pass. The truncated force jumps at r_c, so a stencil that moves a
     pair across the cutoff at some step adds a jump the derivative does not have; h = 1e-4 shows this at the
     1e-5..1e-2 level, and the derivative is checked at the smaller h where the stencil is clean (relative error
-    < 1e-6). On the 32,000-atom workload a sigma stencil moves pairs across r_c at every practical h (1e-2 at
-    h = 1e-8), so sigma is checked on the 864-atom system; the GPU gradients there and on the full workload equal
-    the CPU adjoint's bit for bit (test above), which the CPU tests check against central differences."""
+    < 1e-6). On the 32,000-atom workload only epsilon has such an h: a sigma or position stencil moves pairs across
+    r_c at every h down to 1e-7 (errors 1e-4..1e-2), and below that the difference quotient of |J| ~ 2e5 is
+    rounding noise (4e-4 at h = 1e-8). So sigma and positions are checked on the 864-atom system; the GPU gradients
+    there and on the full workload equal the CPU adjoint's bit for bit (test above), which the CPU tests check
+    against central differences."""
     st, gpu, _ = engines(md, oracle, cells, 0.8442, 1.0, steps, 20)
     rng = np.random.default_rng(3)
     dp = np.zeros_like(st.pos)
