@@ -526,7 +526,8 @@ def run_gpu_arm(a):
                          "frac": achieved / peak, "traffic": None if tpa is None else tpa * n,
                          "kernel": {"fp64": "k_force_fp64", "fx64": "k_force_fx64_rows"}.get(a.precision, "k_force_fp32"),
                          "force_variant": {0: "global gathers", 1: "shared-memory tiles",
-                                           2: "global gathers, rows prefetched"}.get(variant, str(variant)),
+                                           2: "global gathers, rows prefetched",
+                                           3: "global gathers, rows prefetched, registers capped"}.get(variant, str(variant)),
                          "kernel_ms": kernel_s * 1e3,
                          "algorithmic_bytes_per_atom": bytes_per_atom, "peak_source": peak_src},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),

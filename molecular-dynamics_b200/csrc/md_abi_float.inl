@@ -127,14 +127,15 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
         const unsigned g = blocks_for(n, 128);
         if (nl->use_cells) {
             // variant 0: global gathers (k_force_fp32_rows); 1: shared-memory tile; 2: global gathers with the rows
-            // prefetched a group ahead (all the same bits)
+            // prefetched a group ahead; 3: as 2 with capped registers (all the same bits)
             if (!frames_fresh) MD_TRY(frames_async(s, nl));
             const TileGeom& tg = nl->tiles_geom;
             const CellOffsets offs = cell_offsets(nl, s);
             const size_t smem = sizeof(float4) * (tg.max_staged + 1);
             auto launch = [&](int variant, bool with_kick, bool energy) -> md_status {
                 const KickArgs ka{with_kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
-                auto go = [&](auto rows_kernel, auto tile_kernel, auto prefetch_kernel) -> md_status {
+                auto go = [&](auto rows_kernel, auto tile_kernel, auto prefetch_kernel,
+                              auto capped_kernel) -> md_status {
                     if (variant == 1) {
                         if (smem > kSmemNoOptIn)
                             MD_CUDA(cudaFuncSetAttribute(tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -145,6 +146,9 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
                     } else if (variant == 2) {
                         prefetch_kernel<<<g, 128, 0, s->stream>>>(nl->frames.p, s->pos.p, n, s->box, lj, offs,
                                                                   nl->rows.p, nl->cap, nl->counts.p, s->force.p, acc, ka);
+                    } else if (variant == 3) {
+                        capped_kernel<<<g, 128, 0, s->stream>>>(nl->frames.p, s->pos.p, n, s->box, lj, offs, nl->rows.p,
+                                                                nl->cap, nl->counts.p, s->force.p, acc, ka);
                     } else {
                         rows_kernel<<<g, 128, 0, s->stream>>>(nl->frames.p, s->pos.p, n, s->box, lj, offs, nl->rows.p,
                                                               nl->cap, nl->counts.p, s->force.p, acc, ka);
@@ -154,13 +158,13 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
                 };
                 if (fixed)
                     return energy ? go(k_force_fp32_rows<true, true>, k_force_fp32_tile<true, true>,
-                                       k_force_fp32_rows<true, true, true>)
+                                       k_force_fp32_rows<true, true, true>, k_force_fp32_rows<true, true, true, 8>)
                                   : go(k_force_fp32_rows<true, false>, k_force_fp32_tile<true, false>,
-                                       k_force_fp32_rows<true, false, true>);
+                                       k_force_fp32_rows<true, false, true>, k_force_fp32_rows<true, false, true, 8>);
                 return energy ? go(k_force_fp32_rows<false, true>, k_force_fp32_tile<false, true>,
-                                   k_force_fp32_rows<false, true, true>)
+                                   k_force_fp32_rows<false, true, true>, k_force_fp32_rows<false, true, true, 8>)
                               : go(k_force_fp32_rows<false, false>, k_force_fp32_tile<false, false>,
-                                   k_force_fp32_rows<false, false, true>);
+                                   k_force_fp32_rows<false, false, true>, k_force_fp32_rows<false, false, true, 8>);
             };
             MD_TRY(choose_variant(s, nl, ff->precision, [&](int v) { return launch(v, false, false); }));
             if (want_energy || kick) MD_CUDA(cudaMemsetAsync(ff->fx_acc.p, 0, 4 * sizeof(long long), s->stream));

@@ -62,13 +62,21 @@ __device__ __forceinline__ bool exact_inside(const double4& a, const double4& b,
     return norm2(dx, dy, dz) < rc2;
 }
 
+// The hardware's approximate reciprocal (PTX rcp.approx.ftz.f32: one instruction, within 1 ulp); deterministic,
+// so every kernel that calls it gets the same bits
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // One pair in float with a pinned operation sequence (explicit roundings and FMAs), shared by every float
 // kernel. Adds its force to (gx, gy, gz) and, with kEnergy, its energy, virial and inside count.
 template <bool kEnergy>
 __device__ __forceinline__ void float_pair(float dx, float dy, float dz, bool in, float r2, const FloatLJ& lj,
                                            float& gx, float& gy, float& gz, float& ge, float& gw,
                                            unsigned long long& ins) {
-    const float inv = __frcp_rn(r2);
+    const float inv = rcp_approx(r2);
     const float sr2 = __fmul_rn(lj.sig2, inv);
     const float sr6 = __fmul_rn(__fmul_rn(sr2, sr2), sr2);
     float fr = __fmul_rn(__fmul_rn(fmaf(lj.eps48, sr6, -lj.eps24), sr6), inv);
@@ -195,11 +203,12 @@ __global__ void k_frames(const double4* __restrict__ pos, int n, const int* __re
 
 // Thread per particle over its row with neighbour frames gathered from global memory (L1/L2); rows are read
 // as interleaved uint4, coalesced across the warp.
-// kPrefetch (variant 2): row quads are loaded one group ahead with the streaming cache hint, so the next group's
-// entries are in flight while the current group's frames are gathered, and the streamed rows do not displace
-// the frames from L1/L2. Same arithmetic, same bits.
-template <bool kFixed, bool kEnergy, bool kPrefetch = false>
-__global__ void __launch_bounds__(128) k_force_fp32_rows(const float4* __restrict__ frames,
+// kPrefetch (variants 2 and 3): row quads are loaded one group ahead with the streaming cache hint, so the next
+// group's entries are in flight while the current group's frames are gathered, and the streamed rows do not
+// displace the frames from L1/L2. kMinBlocks > 1 (variant 3) caps the registers so that many blocks stay resident
+// on an SM. Same arithmetic, same bits.
+template <bool kFixed, bool kEnergy, bool kPrefetch = false, int kMinBlocks = 1>
+__global__ void __launch_bounds__(128, kMinBlocks) k_force_fp32_rows(const float4* __restrict__ frames,
                                                          const double4* __restrict__ pos, int n, Box box,
                                                          FloatLJ lj, CellOffsets offs,
                                                          const uint32_t* __restrict__ rows, int cap,

@@ -56,13 +56,13 @@ __device__ __forceinline__ double fixed_separation(const int4& qi, const int4& q
     return __fma_rn(dx, dx, __fma_rn(dy, dy, dmul(dz, dz)));
 }
 
-// One pair's terms in double with a pinned operation sequence: 1/r^2 from the float reciprocal refined by two
-// Newton steps, then F/r = (48 eps sr6 - 24 eps) sr6 / r^2 and E = 4 eps sr6 (sr6 - 1) - shift
+// One pair's terms in double with a pinned operation sequence: 1/r^2 from the approximate float reciprocal
+// refined by two Newton steps (quadratic convergence from ~2^-23 leaves only the double roundings), then F/r = (48 eps sr6 - 24 eps) sr6 / r^2 and E = 4 eps sr6 (sr6 - 1) - shift
 template <bool kEnergy>
 __device__ __forceinline__ void fx64_pair(double dx, double dy, double dz, bool in, double r2, const Fx64LJ& p,
                                           double& gx, double& gy, double& gz, double& ge, double& gw,
                                           unsigned long long& ins) {
-    double inv = static_cast<double>(__frcp_rn(__double2float_rn(r2)));
+    double inv = static_cast<double>(rcp_approx(__double2float_rn(r2)));
     inv = __fma_rn(inv, __fma_rn(-r2, inv, 1.0), inv);
     inv = __fma_rn(inv, __fma_rn(-r2, inv, 1.0), inv);
     const double sr2 = dmul(p.lj.sig2, inv);

@@ -183,16 +183,27 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
         const double4 pi = pos[i];
         const int z = cell_sorted[i] % n;
         const int h = (z - t.z0 + n) % n;
+        // entries are collected four at a time and stored as one 16-byte quad of the interleaved row
         int cnt = 0;
-        auto push = [&](int j, uint32_t code) {
-            if (cnt < bp.cap) rows[row_index(i, cnt, bp.cap)] = static_cast<uint32_t>(j) | (code << kCodeShift);
+        uint4 quad = make_uint4(0, 0, 0, 0);
+        auto put = [&](uint32_t v) {
+            const int k = cnt & 3;
+            if (k == 0) quad.x = v;
+            else if (k == 1) quad.y = v;
+            else if (k == 2) quad.z = v;
+            else quad.w = v;
+            if (k == 3 && cnt < bp.cap)
+                reinterpret_cast<uint4*>(rows)[(static_cast<size_t>(i >> 5) * (bp.cap >> 2) + (cnt >> 2)) * 32 +
+                                               (i & 31)] = quad;
             ++cnt;
         };
-        auto test = [&](int j, int slot, const float4& o) -> bool {
+        auto push = [&](int j, uint32_t code) { put(static_cast<uint32_t>(j) | (code << kCodeShift)); };
+        // qo = q_i + the cell's image offset, hoisted out of the candidate loop (the margin covers the rounding)
+        auto test = [&](int j, int slot, const float4& qo) -> bool {
             const float4 qj = s_q[slot];
-            const float dx = (qi.x - qj.x) + o.x;
-            const float dy = (qi.y - qj.y) + o.y;
-            const float dz = (qi.z - qj.z) + o.z;
+            const float dx = qo.x - qj.x;
+            const float dy = qo.y - qj.y;
+            const float dz = qo.z - qj.z;
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             if (r2 < bp.rl2_lo) return true;
             if (r2 > bp.rl2_hi) return false;
@@ -206,9 +217,10 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
         for (uint32_t code = 0; code < 27; ++code) {
             const int sc = staged_cell(static_cast<int>(code), h, span);
             const float4 o = offs.off[code];
+            const float4 qo = make_float4(qi.x + o.x, qi.y + o.y, qi.z + o.z, 0.0f);
             const int gs = t.gstart[sc], cc = t.count[sc], so = t.off[sc];
             for (int u = max(0, i + 1 - gs); u < cc; ++u)
-                if (test(gs + u, so + u, o)) push(gs + u, code);
+                if (test(gs + u, so + u, qo)) push(gs + u, code);
         }
         const int own = cnt;
         // the j < i that list i, increasing j: cells in increasing cell id
@@ -228,14 +240,16 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
                     const uint32_t code = (ox[a] + 1) * 9 + (oy[b] + 1) * 3 + (oz[d] + 1);
                     const int sc = staged_cell(static_cast<int>(code), h, span);
                     const float4 o = offs.off[code];
+                    const float4 qo = make_float4(qi.x + o.x, qi.y + o.y, qi.z + o.z, 0.0f);
                     const int gs = t.gstart[sc], cc = t.count[sc], so = t.off[sc];
                     const int ue = min(cc, i - gs);
                     for (int u = 0; u < ue; ++u)
-                        if (test(gs + u, so + u, o)) push(gs + u, code);
+                        if (test(gs + u, so + u, qo)) push(gs + u, code);
                 }
         counts[i] = make_int2(own, cnt - own);
+        // sentinels up to a multiple of 8 (which also stores the last partial quad)
         const int padded = (cnt + 7) & ~7;
-        for (int s = cnt; s < padded && s < bp.cap; ++s) rows[row_index(i, s, bp.cap)] = bp.sentinel | (kSentinelCode << kCodeShift);
+        while (cnt < padded) put(bp.sentinel | (kSentinelCode << kCodeShift));
         atomicMax(max_count, padded);
     }
 }
