@@ -497,12 +497,13 @@ __global__ void __launch_bounds__(kTile)
 }
 
 // The float list forces per replica (k_force_fp32_rows and, for replicas under 3 cells per side,
-// k_force_fp32_small), with the same pinned pair sequence and 8-entry groups. Each block covers `apb`
+// k_force_fp32_small), with the same pinned pair sequence and 8-entry groups (kPrefetch: rows one group ahead).
+// Each block covers `apb`
 // consecutive particles of one tile with kTPA threads per particle; thread u of a particle takes groups
 // u, u + kTPA, ... and the threads' fixed-point sums are added as integers, so every (apb, kTPA) gives the same
 // bits (kTPA > 1 only with fixed point). Per-replica sums go to acc[4 r .. 4 r + 3] (energy, virial, inside
 // count, kinetic energy after the fused kick).
-template <bool kFixed, bool kEnergy, int kTPA>
+template <bool kFixed, bool kEnergy, int kTPA, bool kPrefetch = false>
 __global__ void __launch_bounds__(256)
     k_b_force_fp32(const BRep* __restrict__ reps, const int* __restrict__ tile_rep, int apb,
                    const float4* __restrict__ frames, const double4* __restrict__ pos, FloatLJ lj,
@@ -530,9 +531,26 @@ __global__ void __launch_bounds__(256)
         const int groups = (m + 7) >> 3;
         if (d.use_cells) {
             const float4 qi = frames[a];
+            // with kPrefetch (one thread per particle) the next group's row quads are in flight while this
+            // group's frames are gathered, as in k_force_fp32_rows
+            uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
+            if (kPrefetch && sub < groups) {
+                n0 = row_quad_stream(rows, a, 2 * sub, cap);
+                n1 = row_quad_stream(rows, a, 2 * sub + 1, cap);
+            }
             for (int g = sub; g < groups; g += kTPA) {
-                const uint4 e0 = row_quad(rows, a, 2 * g, cap);
-                const uint4 e1 = row_quad(rows, a, 2 * g + 1, cap);
+                uint4 e0, e1;
+                if (kPrefetch) {
+                    e0 = n0;
+                    e1 = n1;
+                    if (g + kTPA < groups) {
+                        n0 = row_quad_stream(rows, a, 2 * (g + kTPA), cap);
+                        n1 = row_quad_stream(rows, a, 2 * (g + kTPA) + 1, cap);
+                    }
+                } else {
+                    e0 = row_quad(rows, a, 2 * g, cap);
+                    e1 = row_quad(rows, a, 2 * g + 1, cap);
+                }
                 const uint32_t ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
                 float gx = 0.f, gy = 0.f, gz = 0.f, ge = 0.f, gw = 0.f;
 #pragma unroll

@@ -57,6 +57,7 @@ struct md_batch {
     std::map<int, std::pair<cudaGraphExec_t, uint64_t>> graphs;  // chunk length -> (graph, kernels in it)
     struct Variant {
         int apb, tpa;
+        bool prefetch;
     };
     std::vector<Variant> variants;
     int variant = 0;
@@ -134,15 +135,16 @@ md_status b_float_forces(md_batch* b, const md_batch::Variant& v, bool kick) {
     const int threads = v.apb * v.tpa;
     double* kv = kick ? b->vel.p : nullptr;
     const double half_dt = 0.5 * b->opt.dt;
-#define MD_B_FORCE(T)                                                                                                 \
-    k_b_force_fp32<kFixed, kEnergy, T><<<grid, threads, 0, b->stream>>>(                                              \
+#define MD_B_FORCE(T, P)                                                                                              \
+    k_b_force_fp32<kFixed, kEnergy, T, P><<<grid, threads, 0, b->stream>>>(                                           \
         b->reps.p, b->tile_rep.p, v.apb, b->frames.p, b->pos.p, b->flj, b->rows.p, b->cap, b->counts.p, b->force.p, \
         b->acc.p, kv, b->mass.p, half_dt)
     if (v.tpa == 1) {
-        MD_B_FORCE(1);
+        if (v.prefetch) MD_B_FORCE(1, true);
+        else MD_B_FORCE(1, false);
     } else if constexpr (kFixed) {
-        if (v.tpa == 2) MD_B_FORCE(2);
-        else MD_B_FORCE(4);
+        if (v.tpa == 2) MD_B_FORCE(2, false);
+        else MD_B_FORCE(4, false);
     } else {
         return fail(MD_ERR_INVALID, "float accumulation runs one thread per particle");
     }
@@ -663,11 +665,12 @@ md_status md_batch_create(int device, int replicas, const int64_t* n_atoms, cons
     }
     // force kernel variants: (particles per block, threads per particle)
     if (o.precision == MD_PREC_FP32FX)
-        b->variants = {{128, 1}, {64, 1}, {32, 1}, {64, 2}, {128, 2}, {32, 4}, {64, 4}};
+        b->variants = {{128, 1, false}, {64, 1, false}, {32, 1, false}, {64, 2, false}, {128, 2, false},
+                       {32, 4, false}, {64, 4, false}, {128, 1, true}, {64, 1, true}};
     else if (o.precision == MD_PREC_FP32)
-        b->variants = {{128, 1}, {64, 1}, {32, 1}};
+        b->variants = {{128, 1, false}, {64, 1, false}, {32, 1, false}, {128, 1, true}, {64, 1, true}};
     else
-        b->variants = {{128, 1}};
+        b->variants = {{128, 1, false}};
     if (st == MD_OK) st = b_initial_build(b);
     if (st == MD_OK) st = b_autotune(b);
     if (st == MD_OK) st = b_clear_acc(b);
