@@ -66,8 +66,6 @@ def args_parse():
     p.add_argument("--replicas", type=int, default=512)
     p.add_argument("--adjoint-steps", type=int, default=200,
                    help="trajectory length of the differentiation workload (N = 32,000; 0: skip)")
-    p.add_argument("--build-variant", type=int, default=-1, choices=[-1, 0, 1],
-                   help="tiled list-build kernel: -1 autotune, 0 thread per particle, 1 warp per cell with masks")
     p.add_argument("--profile-region", action="store_true",
                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return p.parse_args()
@@ -387,7 +385,6 @@ def run_gpu_arm(a):
     dt = 0.005
     s = md.fcc_system(a.cells, a.density, a.temperature, seed=42 + rank, device=local)
     nl = md.NeighbourList(2.5, 0.3)
-    nl.set_build_variant(a.build_variant)
     ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)
     integ = md.VelocityVerletIntegrator(dt)
     nl.build(s)

@@ -154,11 +154,6 @@ md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_c
  * bits. md_nlist_force_variant reports the variant in use (-1 until the first force call). */
 md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant);
 md_status md_nlist_force_variant(const md_nlist* nl, int precision, int* variant);
-/* Tiled list-build kernel: -1 autotunes (the first tiled build times both and keeps the faster), 0 pins a thread
- * per particle, 1 pins a warp per cell with partner bitmasks (cells of up to 64 particles; larger cells use 0).
- * Both write the same rows. md_nlist_build_variant reports the choice (-1 until a tiled build has run). */
-md_status md_nlist_set_build_variant(md_nlist* nl, int variant);
-md_status md_nlist_build_variant(const md_nlist* nl, int* variant);
 /* Layout of the last build (diagnostics): whether the shared-memory tile kernels are in use, the segment
  * length in cells, segments per cell column, the largest staged tile (particles) and the row capacity.
  * Any pointer may be NULL. */

@@ -156,9 +156,6 @@ struct md_nlist {
     DevBuf<int4> iframes;   // fixed-point frames of MD_PREC_FX64 (n)
     bool use_tiles = false; // shared-memory tile kernels (3+ cells per side and tiles that fit)
     TileGeom tiles_geom{};
-    int max_occ = 0;         // largest cell occupancy of the last build (picks the list-build kernel)
-    int build_variant = -1;  // tiled list build: 0 thread per atom, 1 warp per cell with masks, -1 untuned
-    int build_pinned = -1;   // set by md_nlist_set_build_variant
     int variant[4] = {-1, -1, -1, -1};  // force kernel per precision (0 global gathers, 1 tile; -1 untuned)
     int pinned[4] = {-1, -1, -1, -1};   // set by md_nlist_set_force_variant
     int rebuilds = 0;
@@ -326,7 +323,6 @@ md_status tile_geometry(md_nlist* nl, md_system* s, bool* use) {
         MD_CHECK_LAUNCH();
         int staged = 0;
         MD_CUDA(cudaMemcpyAsync(&staged, nl->flags.p + 2, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-        MD_CUDA(cudaMemcpyAsync(&nl->max_occ, nl->grid.max_occ.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
         MD_TRY(sync(s));
         g.max_staged = std::max(staged, 1);
         if (staged <= 3072 || kk == 1) {
@@ -389,52 +385,14 @@ md_status nlist_build(md_nlist* nl, md_system* s) {
             const double margin = 1e-5 * nl->rl2 + 1e-4;  // float r^2 error is below 1e-5 here
             BuildParams bp{nl->rl2, static_cast<float>(nl->rl2 - margin), static_cast<float>(nl->rl2 + margin),
                            nl->cap, static_cast<uint32_t>(n)};
-            auto launch = [&](int v) -> md_status {
-                if (v == 1) {
-                    const size_t smem = sizeof(float4) * (tg.max_staged + 1) + mask_smem_bytes();
-                    if (smem > kSmemNoOptIn)
-                        MD_CUDA(cudaFuncSetAttribute(k_nlist_build_masks, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     static_cast<int>(smem)));
-                    k_nlist_build_masks<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
-                        nl->frames.p, s->pos.p, nl->grid.start.p, tg, bp, cell_offsets(nl, s), nl->rows.p,
-                        nl->counts.p, nl->flags.p + 1);
-                } else {
-                    const size_t smem = sizeof(float4) * tg.max_staged;
-                    if (smem > kSmemNoOptIn)
-                        MD_CUDA(cudaFuncSetAttribute(k_nlist_build_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     static_cast<int>(smem)));
-                    k_nlist_build_tile<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
-                        nl->frames.p, s->pos.p, nl->grid.start.p, nl->cell_sorted.p, tg, bp, cell_offsets(nl, s),
-                        nl->rows.p, nl->counts.p, nl->flags.p + 1);
-                }
-                MD_CHECK_LAUNCH();
-                return MD_OK;
-            };
-            // the warp-per-cell build holds cells of up to kMaskChunks * 32 particles; both give the same rows,
-            // so the first tiled build times both and keeps the faster
-            const bool masks_ok = nl->max_occ <= kMaskChunks * 32;
-            int v = nl->build_pinned >= 0 ? nl->build_pinned : nl->build_variant;
-            if (v == 1 && !masks_ok) v = 0;
-            if (v < 0) {
-                if (!masks_ok) {
-                    v = 0;
-                } else {
-                    cudaEvent_t e[3];
-                    for (auto& ev : e) MD_CUDA(cudaEventCreate(&ev));
-                    MD_CUDA(cudaEventRecord(e[0], s->stream));
-                    MD_TRY(launch(0));
-                    MD_CUDA(cudaEventRecord(e[1], s->stream));
-                    MD_TRY(launch(1));
-                    MD_CUDA(cudaEventRecord(e[2], s->stream));
-                    MD_CUDA(cudaEventSynchronize(e[2]));
-                    float t0 = 0.f, t1 = 0.f;
-                    MD_CUDA(cudaEventElapsedTime(&t0, e[0], e[1]));
-                    MD_CUDA(cudaEventElapsedTime(&t1, e[1], e[2]));
-                    for (auto& ev : e) cudaEventDestroy(ev);
-                    nl->build_variant = v = t1 < t0 ? 1 : 0;
-                }
-            }
-            MD_TRY(launch(v));
+            const size_t smem = sizeof(float4) * tg.max_staged;
+            if (smem > kSmemNoOptIn)
+                MD_CUDA(cudaFuncSetAttribute(k_nlist_build_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem)));
+            k_nlist_build_tile<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
+                nl->frames.p, s->pos.p, nl->grid.start.p, nl->cell_sorted.p, tg, bp, cell_offsets(nl, s), nl->rows.p,
+                nl->counts.p, nl->flags.p + 1);
+            MD_CHECK_LAUNCH();
         } else if (n > 0) {
             ListGeom geo{s->box, nl->rl2, nl->grid.ncps, nl->use_cells ? 1 : 0, nl->cap, sentinel};
             k_nlist_build<<<blocks_for(n, 128), 128, 0, s->stream>>>(s->pos.p, n, geo, nl->cell_sorted.p,
@@ -1138,19 +1096,6 @@ md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant) {
         return fail(MD_ERR_INVALID, "md_nlist_set_force_variant: bad arguments");
     nl->pinned[precision] = variant;
     nl->variant[precision] = -1;
-    return MD_OK;
-}
-
-md_status md_nlist_set_build_variant(md_nlist* nl, int variant) {
-    if (!nl || variant < -1 || variant > 1) return fail(MD_ERR_INVALID, "md_nlist_set_build_variant: bad arguments");
-    nl->build_pinned = variant;
-    nl->build_variant = -1;
-    return MD_OK;
-}
-
-md_status md_nlist_build_variant(const md_nlist* nl, int* variant) {
-    if (!nl || !variant) return fail(MD_ERR_INVALID, "md_nlist_build_variant: bad arguments");
-    *variant = nl->build_pinned >= 0 ? nl->build_pinned : nl->build_variant;
     return MD_OK;
 }
 

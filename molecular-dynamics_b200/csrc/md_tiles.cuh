@@ -240,131 +240,6 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
     }
 }
 
-// NeighbourList::build on a tile with one warp per home cell and no divergence in the distance tests.
-// Phase 1: for every home atom h of the warp's cell (up to 32 at a time) and every candidate cell, the lanes hold
-// 32 of that cell's staged frames and test them against h together; the ballot is h's 32-bit mask of partners in
-// that cell (the same float prefilter and exact double test near r_l as k_nlist_build_tile, so the same pairs).
-// Phase 2: each lane writes its home atom's row from its masks: own pairs (j > i) in candidate order, then the
-// j < i in increasing cell id, increasing j inside a cell (bits ascending) -- the rows of k_nlist_build_tile.
-// Cells of up to kMaskChunks * 32 particles; the host uses k_nlist_build_tile when a cell holds more.
-constexpr int kMaskChunks = 2;
-constexpr int kMaskWarps = kTileThreads / 32;
-inline size_t mask_smem_bytes() { return sizeof(uint32_t) * kMaskWarps * 32 * 27 * kMaskChunks; }
-
-__global__ void __launch_bounds__(kTileThreads) k_nlist_build_masks(
-    const float4* __restrict__ frames, const double4* __restrict__ pos, const int* __restrict__ cell_start,
-    TileGeom g, BuildParams bp, CellOffsets offs, uint32_t* __restrict__ rows, int2* __restrict__ counts,
-    int* __restrict__ max_count) {
-    extern __shared__ float4 s_q[];
-    __shared__ TileTables t;
-    tile_tables(g, cell_start, t);
-    if (t.total > g.max_staged) {  // the host's bound was wrong: report a full row so it rebuilds bigger
-        if (threadIdx.x == 0) atomicMax(max_count, 1 << 30);
-        return;
-    }
-    stage_tile(frames, s_q, t);
-    cp_async_wait();
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t* masks = reinterpret_cast<uint32_t*>(s_q + g.max_staged + 1) + warp * 32 * 27 * kMaskChunks;
-    const int n = g.ncps;
-    const int span = t.kk + 2;
-    const float far = kSentinelCoord;
-    for (int h = warp; h < t.kk; h += kMaskWarps) {
-        const int hc = staged_cell(13, h, span);
-        const int hgs = t.gstart[hc], hcount = t.count[hc], hso = t.off[hc];
-        const int z = (t.z0 + h) % n;
-        for (int hb = 0; hb < hcount; hb += 32) {
-            const int nh = min(32, hcount - hb);
-            // phase 1: masks[t][code][k] for the home atoms hb + t
-            for (int code = 0; code < 27; ++code) {
-                const int sc = staged_cell(code, h, span);
-                const int gs = t.gstart[sc], cc = t.count[sc], so = t.off[sc];
-                const float4 o = offs.off[code];
-                for (int k = 0; k * 32 < cc && k < kMaskChunks; ++k) {
-                    const int u = k * 32 + lane;
-                    const bool valid = u < cc;
-                    const float4 qj = valid ? s_q[so + u] : make_float4(far, far, far, 0.0f);
-                    for (int a = 0; a < nh; ++a) {
-                        const float4 qh = s_q[hso + hb + a];
-                        const float dx = (qh.x + o.x) - qj.x;
-                        const float dy = (qh.y + o.y) - qj.y;
-                        const float dz = (qh.z + o.z) - qj.z;
-                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        bool in = r2 < bp.rl2_lo;
-                        const bool shell = valid && !in && r2 <= bp.rl2_hi;
-                        if (__any_sync(0xffffffffu, shell) && shell) {  // thin shell: the reference's double test
-                            const double4 pi = pos[hgs + hb + a], pj = pos[gs + u];
-                            const double ex = min_image(dsub(pi.x, pj.x), g.box);
-                            const double ey = min_image(dsub(pi.y, pj.y), g.box);
-                            const double ez = min_image(dsub(pi.z, pj.z), g.box);
-                            in = norm2(ex, ey, ez) < bp.rl2;
-                        }
-                        const uint32_t m = __ballot_sync(0xffffffffu, in);
-                        if (lane == a) masks[(a * 27 + code) * kMaskChunks + k] = m;
-                    }
-                }
-            }
-            __syncwarp();
-            // phase 2: lane a writes the row of home atom i = hgs + hb + a
-            if (lane < nh) {
-                const int a = lane;
-                const int i = hgs + hb + a;
-                int cnt = 0;
-                auto emit = [&](uint32_t m, int base, uint32_t code) {
-                    while (m) {
-                        const int b = __ffs(m) - 1;
-                        m &= m - 1;
-                        if (cnt < bp.cap)
-                            rows[row_index(i, cnt, bp.cap)] = static_cast<uint32_t>(base + b) | (code << kCodeShift);
-                        ++cnt;
-                    }
-                };
-                // bits of chunk base `base` with j > i, and with j < i
-                auto above = [&](uint32_t m, int base) -> uint32_t {
-                    const int d = i - base;
-                    return d < 0 ? m : (d >= 31 ? 0u : m & ~((2u << d) - 1u));
-                };
-                auto below = [&](uint32_t m, int base) -> uint32_t {
-                    const int d = i - base;
-                    return d <= 0 ? 0u : (d >= 32 ? m : m & ((1u << d) - 1u));
-                };
-                for (uint32_t code = 0; code < 27; ++code) {
-                    const int sc = staged_cell(static_cast<int>(code), h, span);
-                    const int gs = t.gstart[sc], cc = t.count[sc];
-                    for (int k = 0; k * 32 < cc && k < kMaskChunks; ++k)
-                        emit(above(masks[(a * 27 + code) * kMaskChunks + k], gs + 32 * k), gs + 32 * k, code);
-                }
-                const int own = cnt;
-                int ox[3], oy[3], oz[3];
-                auto asc = [n](int c, int* d) {
-                    if (c == 0) { d[0] = 0; d[1] = 1; d[2] = -1; }
-                    else if (c == n - 1) { d[0] = 1; d[1] = -1; d[2] = 0; }
-                    else { d[0] = -1; d[1] = 0; d[2] = 1; }
-                };
-                asc(t.cx, ox);
-                asc(t.cy, oy);
-                asc(z, oz);
-                for (int p = 0; p < 3; ++p)
-                    for (int q = 0; q < 3; ++q)
-                        for (int r = 0; r < 3; ++r) {
-                            const uint32_t code = (ox[p] + 1) * 9 + (oy[q] + 1) * 3 + (oz[r] + 1);
-                            const int sc = staged_cell(static_cast<int>(code), h, span);
-                            const int gs = t.gstart[sc], cc = t.count[sc];
-                            for (int k = 0; k * 32 < cc && k < kMaskChunks; ++k)
-                                emit(below(masks[(a * 27 + code) * kMaskChunks + k], gs + 32 * k), gs + 32 * k, code);
-                        }
-                counts[i] = make_int2(own, cnt - own);
-                const int padded = (cnt + 7) & ~7;
-                for (int s2 = cnt; s2 < padded && s2 < bp.cap; ++s2)
-                    rows[row_index(i, s2, bp.cap)] = bp.sentinel | (kSentinelCode << kCodeShift);
-                atomicMax(max_count, padded);
-            }
-            __syncwarp();
-        }
-    }
-}
-
 // ---- float forces -----------------------------------------------------------------------------------------
 
 // Per-block table entry for (home z offset, code): image offset -d * cell in x, y, z and the shared slot delta

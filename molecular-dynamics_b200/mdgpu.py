@@ -67,7 +67,6 @@ def _load():
         "md_nlist_info": (_I, [_P, _PU64, _PI, _PI, _PI]),
         "md_nlist_layout": (_I, [_P, _PI, _PI, _PI, _PI, _PI]),
         "md_nlist_set_force_variant": (_I, [_P, _I, _I]), "md_nlist_force_variant": (_I, [_P, _I, _PI]),
-        "md_nlist_set_build_variant": (_I, [_P, _I]), "md_nlist_build_variant": (_I, [_P, _PI]),
         "md_nlist_download": (_I, [_P, _PU64, _PU64, _PU64, _PU64]),
         "md_forcefield_create": (_I, [_D, _D, _D, _PP]), "md_forcefield_destroy": (_I, [_P]),
         "md_forcefield_shift": (_I, [_P, _PD]), "md_forcefield_set_precision": (_I, [_P, _I]),
@@ -371,15 +370,6 @@ class NeighbourList:
     def force_variant(self, precision: int) -> int:
         v = C.c_int()
         _check(LIB.md_nlist_force_variant(self.h, precision, C.byref(v)))
-        return v.value
-
-    def set_build_variant(self, variant: int):
-        """Tiled list build: -1 autotune, 0 thread per particle, 1 warp per cell with bitmasks (same rows)."""
-        _check(LIB.md_nlist_set_build_variant(self.h, variant))
-
-    def build_variant(self) -> int:
-        v = C.c_int()
-        _check(LIB.md_nlist_build_variant(self.h, C.byref(v)))
         return v.value
 
     def layout(self) -> dict:

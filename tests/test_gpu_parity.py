@@ -443,27 +443,3 @@ def test_frame_by_id_inverts_the_list_permutation(md):
     assert np.array_equal(frame[:, :3], st["pos"][where, :3])
     assert np.array_equal(frame[:, 3:], st["vel"][:, where].T)
     assert np.array_equal(s.frame_by_id(), frame)
-
-
-@pytest.mark.parametrize("cells,density,temperature", [(8, 0.8442, 1.2), (30, 0.8442, 0.71), (24, 1.0, 2.0)])
-def test_list_build_kernels_agree(md, cells, density, temperature):
-    """The two tiled list builds (a thread per particle; a warp per cell with partner bitmasks) write the same
-    lists: the reference's own pairs, reverse pairs and their order (src/NeighbourList.cpp:55-134)."""
-    base = md.fcc_system(cells, density, temperature, seed=9)
-    nl0 = md.NeighbourList(2.5, 0.3)
-    nl0.build(base)
-    md.VelocityVerletIntegrator(0.005).run(base, md.LennardJonesForceField(1.0, 1.0, 2.5), nl0, 40, record=False)
-    st = base.download()
-    lists = []
-    for variant in (0, 1):
-        s = md.System.from_arrays(st["pos"], base.box, vel=st["vel"])
-        nl = md.NeighbourList(2.5, 0.3, reverse_index=True)
-        nl.set_build_variant(variant)
-        nl.build(s)
-        if nl.layout()["use_tiles"]:
-            assert nl.build_variant() == variant
-        lists.append((nl.download(), s.download()["ids"]))
-    (la, ia), (lb, ib) = lists
-    assert np.array_equal(ia, ib)
-    for k in ("offsets", "neighbours", "rev_offsets", "rev_pairs"):
-        assert np.array_equal(la[k], lb[k]), k
