@@ -188,14 +188,15 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
             if (cnt < bp.cap) rows[row_index(i, cnt, bp.cap)] = static_cast<uint32_t>(j) | (code << kCodeShift);
             ++cnt;
         };
-        auto test = [&](int j, int slot, const float4& o) -> bool {
+        // qo = q_i + the cell's image offset, hoisted out of the candidate loop (the margin covers the rounding)
+        auto test = [&](int j, int slot, const float4& qo) -> bool {
             const float4 qj = s_q[slot];
-            const float dx = (qi.x - qj.x) + o.x;
-            const float dy = (qi.y - qj.y) + o.y;
-            const float dz = (qi.z - qj.z) + o.z;
+            const float dx = qo.x - qj.x;
+            const float dy = qo.y - qj.y;
+            const float dz = qo.z - qj.z;
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             if (r2 < bp.rl2_lo) return true;
-            if (r2 > bp.rl2_hi) return false;
+            if (!(r2 <= bp.rl2_hi)) return false;
             const double4 pj = pos[j];  // thin shell: the reference's exact double test
             const double ex = min_image(dsub(pi.x, pj.x), g.box);
             const double ey = min_image(dsub(pi.y, pj.y), g.box);
@@ -206,9 +207,11 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
         for (uint32_t code = 0; code < 27; ++code) {
             const int sc = staged_cell(static_cast<int>(code), h, span);
             const float4 o = offs.off[code];
+            const float4 qo = make_float4(qi.x + o.x, qi.y + o.y, qi.z + o.z, 0.0f);
             const int gs = t.gstart[sc], cc = t.count[sc], so = t.off[sc];
+#pragma unroll 4
             for (int u = max(0, i + 1 - gs); u < cc; ++u)
-                if (test(gs + u, so + u, o)) push(gs + u, code);
+                if (test(gs + u, so + u, qo)) push(gs + u, code);
         }
         const int own = cnt;
         // the j < i that list i, increasing j: cells in increasing cell id
@@ -228,10 +231,12 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
                     const uint32_t code = (ox[a] + 1) * 9 + (oy[b] + 1) * 3 + (oz[d] + 1);
                     const int sc = staged_cell(static_cast<int>(code), h, span);
                     const float4 o = offs.off[code];
+                    const float4 qo = make_float4(qi.x + o.x, qi.y + o.y, qi.z + o.z, 0.0f);
                     const int gs = t.gstart[sc], cc = t.count[sc], so = t.off[sc];
                     const int ue = min(cc, i - gs);
+#pragma unroll 4
                     for (int u = 0; u < ue; ++u)
-                        if (test(gs + u, so + u, o)) push(gs + u, code);
+                        if (test(gs + u, so + u, qo)) push(gs + u, code);
                 }
         counts[i] = make_int2(own, cnt - own);
         const int padded = (cnt + 7) & ~7;
