@@ -382,10 +382,16 @@ __global__ void __launch_bounds__(kTile)
             const float4 qi = frames[a];
             const float cellf = static_cast<float>(d.cell);
             const int* st = start + d.cell_off + r;
-            auto take = [&](int j, uint32_t code) {
-                float dx, dy, dz;
-                const float r2 = float_separation(qi, frames[j], code_offset(static_cast<int>(code), cellf), dx, dy, dz);
+            // qo = q_i + the cell's image offset, computed once per candidate cell (the margin covers the rounding)
+            auto take = [&](int j, uint32_t code, const float4& qo) {
+                const float4 qj = frames[j];
+                const float dx = qo.x - qj.x, dy = qo.y - qj.y, dz = qo.z - qj.z;
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                 if (r2 < bp.lo || (r2 <= bp.hi && within_rl(pi, pos[j], d.box, bp.rl2))) push(j, code);
+            };
+            auto shifted = [&](uint32_t code) {
+                const float4 o = code_offset(static_cast<int>(code), cellf);
+                return make_float4(qi.x + o.x, qi.y + o.y, qi.z + o.z, 0.0f);
             };
             const int nc = d.ncps;
             const int c = cell_sorted[a];
@@ -398,7 +404,8 @@ __global__ void __launch_bounds__(kTile)
                         const int cell = (x * nc + y) * nc + (cz + dz + nc) % nc;
                         const uint32_t code = (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
                         const int e = st[cell + 1];
-                        for (int j = st[cell] > a + 1 ? st[cell] : a + 1; j < e; ++j) take(j, code);
+                        const float4 qo = shifted(code);
+                        for (int j = st[cell] > a + 1 ? st[cell] : a + 1; j < e; ++j) take(j, code, qo);
                     }
                 }
             }
@@ -415,7 +422,8 @@ __global__ void __launch_bounds__(kTile)
                         const int cell = (x * nc + y) * nc + (cz + oz[q] + nc) % nc;
                         const uint32_t code = (ox[u] + 1) * 9 + (oy[v] + 1) * 3 + (oz[q] + 1);
                         const int e = st[cell + 1] < a ? st[cell + 1] : a;
-                        for (int j = st[cell]; j < e; ++j) take(j, code);
+                        const float4 qo = shifted(code);
+                        for (int j = st[cell]; j < e; ++j) take(j, code, qo);
                     }
                 }
             }
