@@ -154,6 +154,11 @@ md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_c
  * bits. md_nlist_force_variant reports the variant in use (-1 until the first force call). */
 md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant);
 md_status md_nlist_force_variant(const md_nlist* nl, int precision, int* variant);
+/* List build kernel: -1 uses the shared-memory tile build wherever the list has tiles, 0 pins one thread per
+ * particle over global memory, 1 pins the tile build (while the list has tiles). Both write the same rows.
+ * md_nlist_build_variant reports the kernel of the last build (-1 before the first). */
+md_status md_nlist_set_build_variant(md_nlist* nl, int variant);
+md_status md_nlist_build_variant(const md_nlist* nl, int* variant);
 /* Layout of the last build (diagnostics): whether the shared-memory tile kernels are in use, the segment
  * length in cells, segments per cell column, the largest staged tile (particles) and the row capacity.
  * Any pointer may be NULL. */

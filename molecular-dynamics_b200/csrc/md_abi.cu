@@ -156,6 +156,8 @@ struct md_nlist {
     DevBuf<int4> iframes;   // fixed-point frames of MD_PREC_FX64 (n)
     bool use_tiles = false; // shared-memory tile kernels (3+ cells per side and tiles that fit)
     TileGeom tiles_geom{};
+    int build_kernel = -1;  // list build of the last rebuild: 0 thread per particle, 1 tiles
+    int build_pin = -1;     // set by md_nlist_set_build_variant (-1: tiles where available)
     int variant[4] = {-1, -1, -1, -1};  // force kernel per precision (0 global gathers, 1 tile; -1 untuned)
     int pinned[4] = {-1, -1, -1, -1};   // set by md_nlist_set_force_variant
     int rebuilds = 0;
@@ -380,7 +382,7 @@ md_status nlist_build(md_nlist* nl, md_system* s) {
     for (int attempt = 0; attempt < 4; ++attempt) {
         MD_CUDA(nl->rows.reserve(row_buffer_entries(n, nl->cap)));
         MD_CUDA(cudaMemsetAsync(nl->flags.p, 0, 4 * sizeof(int), s->stream));
-        if (n > 0 && nl->use_tiles) {
+        if (n > 0 && nl->use_tiles && nl->build_pin != 0) {
             const TileGeom& tg = nl->tiles_geom;
             const double margin = 1e-5 * nl->rl2 + 1e-4;  // float r^2 error is below 1e-5 here
             BuildParams bp{nl->rl2, static_cast<float>(nl->rl2 - margin), static_cast<float>(nl->rl2 + margin),
@@ -393,12 +395,14 @@ md_status nlist_build(md_nlist* nl, md_system* s) {
                 nl->frames.p, s->pos.p, nl->grid.start.p, nl->cell_sorted.p, tg, bp, cell_offsets(nl, s), nl->rows.p,
                 nl->counts.p, nl->flags.p + 1);
             MD_CHECK_LAUNCH();
+            nl->build_kernel = 1;
         } else if (n > 0) {
             ListGeom geo{s->box, nl->rl2, nl->grid.ncps, nl->use_cells ? 1 : 0, nl->cap, sentinel};
             k_nlist_build<<<blocks_for(n, 128), 128, 0, s->stream>>>(s->pos.p, n, geo, nl->cell_sorted.p,
                                                                       nl->grid.start.p, nl->rows.p, nl->counts.p,
                                                                       nl->flags.p + 1);
             MD_CHECK_LAUNCH();
+            nl->build_kernel = 0;
         }
         int maxrow = 0;
         MD_CUDA(cudaMemcpyAsync(&maxrow, nl->flags.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
@@ -1103,6 +1107,18 @@ md_status md_nlist_force_variant(const md_nlist* nl, int precision, int* variant
     if (!nl || !variant || precision < MD_PREC_FP64 || precision > MD_PREC_FX64)
         return fail(MD_ERR_INVALID, "md_nlist_force_variant: bad arguments");
     *variant = nl->variant[precision];
+    return MD_OK;
+}
+
+md_status md_nlist_set_build_variant(md_nlist* nl, int variant) {
+    if (!nl || variant < -1 || variant > 1) return fail(MD_ERR_INVALID, "md_nlist_set_build_variant: bad arguments");
+    nl->build_pin = variant;
+    return MD_OK;
+}
+
+md_status md_nlist_build_variant(const md_nlist* nl, int* variant) {
+    if (!nl || !variant) return fail(MD_ERR_INVALID, "md_nlist_build_variant: bad arguments");
+    *variant = nl->build_kernel;
     return MD_OK;
 }
 

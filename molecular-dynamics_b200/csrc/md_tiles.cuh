@@ -162,6 +162,15 @@ struct BuildParams {
     uint32_t sentinel;     // index of the sentinel particle (n)
 };
 
+// The reference's list test in double (src/NeighbourList.cpp:38-52), kept out of line: only candidates within
+// float rounding of r_l reach it
+__device__ __noinline__ bool exact_within(const double4& pi, const double4& pj, const Box& box, double rl2) {
+    const double ex = min_image(dsub(pi.x, pj.x), box);
+    const double ey = min_image(dsub(pi.y, pj.y), box);
+    const double ez = min_image(dsub(pi.z, pj.z), box);
+    return norm2(ex, ey, ez) < rl2;
+}
+
 __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
     const float4* __restrict__ frames, const double4* __restrict__ pos, const int* __restrict__ cell_start,
     const int* __restrict__ cell_sorted, TileGeom g, BuildParams bp, CellOffsets offs, uint32_t* __restrict__ rows,
@@ -184,34 +193,31 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
         const int z = cell_sorted[i] % n;
         const int h = (z - t.z0 + n) % n;
         int cnt = 0;
+        // this particle's interleaved row: entry s at row[(s >> 2) * 128 + (s & 3)]
+        uint32_t* row = rows + static_cast<size_t>(i >> 5) * (bp.cap >> 2) * 128 + (i & 31) * 4;
         auto push = [&](int j, uint32_t code) {
-            if (cnt < bp.cap) rows[row_index(i, cnt, bp.cap)] = static_cast<uint32_t>(j) | (code << kCodeShift);
+            if (cnt < bp.cap) row[(cnt >> 2) * 128 + (cnt & 3)] = static_cast<uint32_t>(j) | (code << kCodeShift);
             ++cnt;
         };
         // qo = q_i + the cell's image offset, hoisted out of the candidate loop (the margin covers the rounding)
-        auto test = [&](int j, int slot, const float4& qo) -> bool {
-            const float4 qj = s_q[slot];
+        auto test = [&](int j, const float4& qj, const float4& qo) -> bool {
             const float dx = qo.x - qj.x;
             const float dy = qo.y - qj.y;
             const float dz = qo.z - qj.z;
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             if (r2 < bp.rl2_lo) return true;
             if (!(r2 <= bp.rl2_hi)) return false;
-            const double4 pj = pos[j];  // thin shell: the reference's exact double test
-            const double ex = min_image(dsub(pi.x, pj.x), g.box);
-            const double ey = min_image(dsub(pi.y, pj.y), g.box);
-            const double ez = min_image(dsub(pi.z, pj.z), g.box);
-            return norm2(ex, ey, ez) < bp.rl2;
+            return exact_within(pi, pos[j], g.box, bp.rl2);  // thin shell: the reference's exact double test
         };
         // own pairs: 27 cells in (dx, dy, dz) order, increasing j inside each (src/CellList.cpp:55-83)
         for (uint32_t code = 0; code < 27; ++code) {
             const int sc = staged_cell(static_cast<int>(code), h, span);
             const float4 o = offs.off[code];
             const float4 qo = make_float4(qi.x + o.x, qi.y + o.y, qi.z + o.z, 0.0f);
-            const int gs = t.gstart[sc], cc = t.count[sc], so = t.off[sc];
-#pragma unroll 4
+            const int gs = t.gstart[sc], cc = t.count[sc];
+            const float4* q = s_q + t.off[sc];
             for (int u = max(0, i + 1 - gs); u < cc; ++u)
-                if (test(gs + u, so + u, qo)) push(gs + u, code);
+                if (test(gs + u, q[u], qo)) push(gs + u, code);
         }
         const int own = cnt;
         // the j < i that list i, increasing j: cells in increasing cell id
@@ -232,15 +238,15 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
                     const int sc = staged_cell(static_cast<int>(code), h, span);
                     const float4 o = offs.off[code];
                     const float4 qo = make_float4(qi.x + o.x, qi.y + o.y, qi.z + o.z, 0.0f);
-                    const int gs = t.gstart[sc], cc = t.count[sc], so = t.off[sc];
+                    const int gs = t.gstart[sc], cc = t.count[sc];
+                    const float4* q = s_q + t.off[sc];
                     const int ue = min(cc, i - gs);
-#pragma unroll 4
                     for (int u = 0; u < ue; ++u)
-                        if (test(gs + u, so + u, qo)) push(gs + u, code);
+                        if (test(gs + u, q[u], qo)) push(gs + u, code);
                 }
         counts[i] = make_int2(own, cnt - own);
         const int padded = (cnt + 7) & ~7;
-        for (int s = cnt; s < padded && s < bp.cap; ++s) rows[row_index(i, s, bp.cap)] = bp.sentinel | (kSentinelCode << kCodeShift);
+        for (int s = cnt; s < padded && s < bp.cap; ++s) row[(s >> 2) * 128 + (s & 3)] = bp.sentinel | (kSentinelCode << kCodeShift);
         atomicMax(max_count, padded);
     }
 }

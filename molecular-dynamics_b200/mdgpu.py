@@ -67,6 +67,7 @@ def _load():
         "md_nlist_info": (_I, [_P, _PU64, _PI, _PI, _PI]),
         "md_nlist_layout": (_I, [_P, _PI, _PI, _PI, _PI, _PI]),
         "md_nlist_set_force_variant": (_I, [_P, _I, _I]), "md_nlist_force_variant": (_I, [_P, _I, _PI]),
+        "md_nlist_set_build_variant": (_I, [_P, _I]), "md_nlist_build_variant": (_I, [_P, _PI]),
         "md_nlist_download": (_I, [_P, _PU64, _PU64, _PU64, _PU64]),
         "md_forcefield_create": (_I, [_D, _D, _D, _PP]), "md_forcefield_destroy": (_I, [_P]),
         "md_forcefield_shift": (_I, [_P, _PD]), "md_forcefield_set_precision": (_I, [_P, _I]),
@@ -370,6 +371,15 @@ class NeighbourList:
     def force_variant(self, precision: int) -> int:
         v = C.c_int()
         _check(LIB.md_nlist_force_variant(self.h, precision, C.byref(v)))
+        return v.value
+
+    def set_build_variant(self, variant: int):
+        """-1 uses the tile build where the list has tiles; 0 pins one thread per particle, 1 the tiles."""
+        _check(LIB.md_nlist_set_build_variant(self.h, variant))
+
+    def build_variant(self) -> int:
+        v = C.c_int()
+        _check(LIB.md_nlist_build_variant(self.h, C.byref(v)))
         return v.value
 
     def layout(self) -> dict:

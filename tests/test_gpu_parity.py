@@ -426,6 +426,41 @@ def test_force_kernel_variants_agree_bit_for_bit(md, cells, density):
                 assert np.array_equal(sa[k], sb[k]), (prec, k)
 
 
+@pytest.mark.parametrize("cells,density,temperature,skin", [
+    (6, 0.8442, 1.2, 0.3),   # 3 cells per side: every neighbour cell wraps
+    (10, 1.0, 2.0, 0.3),
+    (12, 0.5, 1.2, 0.3),
+    (20, 0.8442, 0.71, 0.3),
+    (12, 1.2, 1.5, 0.3),     # dense: cells above 32 particles
+    (12, 0.8442, 1.2, 1.5),  # long list radius: about 55 particles per cell, two lanes' chunks per cell
+])
+def test_list_build_variants_agree(md, cells, density, temperature, skin):
+    """The shared-memory tile build and the thread-per-particle build write the same rows: the same neighbours,
+    reverse pairs and cell codes (checked through FP32FX trajectories, whose separations use the codes)."""
+    base = md.fcc_system(cells, density, temperature, seed=11)
+    nl0 = md.NeighbourList(2.5, skin)
+    nl0.build(base)
+    md.VelocityVerletIntegrator(0.005).run(base, md.LennardJonesForceField(1.0, 1.0, 2.5), nl0, 40, record=False)
+    st = base.download()
+    out = []
+    for variant in (0, 1):
+        s = md.System.from_arrays(st["pos"], base.box, vel=st["vel"], force=st["force"])
+        nl = md.NeighbourList(2.5, skin, reverse_index=True)
+        nl.set_build_variant(variant)
+        nl.build(s)
+        assert nl.build_variant() == variant or (variant == 1 and not nl.layout()["use_tiles"])
+        L = nl.download()
+        ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=md.PREC_FP32FX)
+        pe, ke, w = md.VelocityVerletIntegrator(0.005).run(s, ff, nl, 10)
+        out.append((L, pe, w, s.download()))
+    for L, pe, w, d in out[1:]:
+        for k in ("offsets", "neighbours", "rev_offsets", "rev_pairs"):
+            assert np.array_equal(L[k], out[0][0][k]), k
+        assert np.array_equal(pe, out[0][1]) and np.array_equal(w, out[0][2])
+        for k in ("pos", "vel", "force"):
+            assert np.array_equal(d[k], out[0][3][k]), k
+
+
 def test_frame_by_id_inverts_the_list_permutation(md):
     """md_system_frame_by_id (writeXyzFrame's data, src/Trajectory.cpp:4-25): after rebuilds have reordered
     the particles, the device gather through the ids equals the host-side inverse permutation."""
