@@ -66,6 +66,8 @@ def args_parse():
     p.add_argument("--replicas", type=int, default=512)
     p.add_argument("--adjoint-steps", type=int, default=200,
                    help="trajectory length of the differentiation workload (N = 32,000; 0: skip)")
+    p.add_argument("--force-variant", type=int, default=-1,
+                   help="list force kernel of the headline run: -1 autotunes, 0-3 pin one (md_nlist_set_force_variant)")
     p.add_argument("--profile-region", action="store_true",
                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return p.parse_args()
@@ -385,6 +387,8 @@ def run_gpu_arm(a):
     dt = 0.005
     s = md.fcc_system(a.cells, a.density, a.temperature, seed=42 + rank, device=local)
     nl = md.NeighbourList(2.5, 0.3)
+    if a.force_variant >= 0:
+        nl.set_force_variant(prec, a.force_variant)
     ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)
     integ = md.VelocityVerletIntegrator(dt)
     nl.build(s)

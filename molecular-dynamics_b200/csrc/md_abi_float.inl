@@ -132,8 +132,9 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
             const TileGeom& tg = nl->tiles_geom;
             const CellOffsets offs = cell_offsets(nl, s);
             const size_t smem = sizeof(float4) * (tg.max_staged + 1);
-            auto launch = [&](int variant, bool with_kick, bool energy) -> md_status {
-                const KickArgs ka{with_kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
+            auto launch = [&](int variant, bool with_kick, bool energy, double* tune_vel = nullptr) -> md_status {
+                const KickArgs ka = tune_vel ? KickArgs{tune_vel, s->mass.p, 0.0}
+                                             : KickArgs{with_kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
                 auto go = [&](auto rows_kernel, auto tile_kernel, auto prefetch_kernel,
                               auto capped_kernel) -> md_status {
                     if (variant == 1) {
@@ -158,15 +159,18 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
                 };
                 if (fixed)
                     return energy ? go(k_force_fp32_rows<true, true>, k_force_fp32_tile<true, true>,
-                                       k_force_fp32_rows<true, true, true>, k_force_fp32_rows<true, true, true, 8>)
+                                       k_force_fp32_rows<true, true, true>, k_force_fp32_rows<true, true, true, 7>)
                                   : go(k_force_fp32_rows<true, false>, k_force_fp32_tile<true, false>,
-                                       k_force_fp32_rows<true, false, true>, k_force_fp32_rows<true, false, true, 8>);
+                                       k_force_fp32_rows<true, false, true>, k_force_fp32_rows<true, false, true, 7>);
                 return energy ? go(k_force_fp32_rows<false, true>, k_force_fp32_tile<false, true>,
-                                   k_force_fp32_rows<false, true, true>, k_force_fp32_rows<false, true, true, 8>)
+                                   k_force_fp32_rows<false, true, true>, k_force_fp32_rows<false, true, true, 7>)
                               : go(k_force_fp32_rows<false, false>, k_force_fp32_tile<false, false>,
-                                   k_force_fp32_rows<false, false, true>, k_force_fp32_rows<false, false, true, 8>);
+                                   k_force_fp32_rows<false, false, true>, k_force_fp32_rows<false, false, true, 7>);
             };
-            MD_TRY(choose_variant(s, nl, ff->precision, [&](int v) { return launch(v, false, false); }));
+            // tune on the kernel the steps run (energy and the fused kick), the kick writing into the reorder
+            // buffer (3n doubles, idle between rebuilds) so the state is untouched
+            MD_CUDA(s->vel2.reserve(3 * static_cast<size_t>(n)));
+            MD_TRY(choose_variant(s, nl, ff->precision, [&](int v) { return launch(v, true, true, s->vel2.p); }));
             if (want_energy || kick) MD_CUDA(cudaMemsetAsync(ff->fx_acc.p, 0, 4 * sizeof(long long), s->stream));
             MD_TRY(profile_mark(s));
             MD_TRY(launch(nl->variant[ff->precision], kick, want_energy));

@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(256)
     const bool active = i < d.n;
     const int a = d.off + i;
     long long e_fx = 0, w_fx = 0, k_fx = 0;
-    unsigned long long ins = 0;
+    unsigned ins = 0;
     FloatAcc<kFixed, kEnergy> acc_i;
     if (active) {
         const int2 c = counts[a];
@@ -559,19 +559,15 @@ __global__ void __launch_bounds__(256)
                     e0 = row_quad(rows, a, 2 * g, cap);
                     e1 = row_quad(rows, a, 2 * g + 1, cap);
                 }
-                const uint32_t ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
-                float gx = 0.f, gy = 0.f, gz = 0.f, ge = 0.f, gw = 0.f;
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const uint32_t e = ent[u];
-                    const int j = static_cast<int>(e & kIndexMask);
-                    float dx, dy, dz;
-                    const float r2 = float_separation(qi, frames[j], s_off[e >> kCodeShift], dx, dy, dz);
-                    bool in = r2 < lj.rc2;
-                    if (fabsf(r2 - lj.rc2) < lj.band) in = exact_inside(pos[a], pos[j], d.box, lj.rc2d);
-                    float_pair<kEnergy>(dx, dy, dz, in, r2, lj, gx, gy, gz, ge, gw, ins);
-                }
-                acc_i.add_group(gx, gy, gz, ge, gw, e_fx, w_fx);
+                const float4* so = s_off;
+                const Box box = d.box;
+                const GroupSums gs = float_group<kEnergy>(
+                    e0, e1, lj,
+                    [=](uint32_t e, float& dx, float& dy, float& dz) {
+                        return float_separation(qi, frames[e & kIndexMask], so[e >> kCodeShift], dx, dy, dz);
+                    },
+                    [=](uint32_t e) { return exact_inside(pos[a], pos[e & kIndexMask], box, lj.rc2d); }, ins);
+                acc_i.add_group(gs.x, gs.y, gs.z, gs.e, gs.w, e_fx, w_fx);
             }
         } else {
             const double4 pi = pos[a];

@@ -71,11 +71,11 @@ __device__ __forceinline__ float rcp_approx(float x) {
 }
 
 // One pair in float with a pinned operation sequence (explicit roundings and FMAs), shared by every float
-// kernel. Adds its force to (gx, gy, gz) and, with kEnergy, its energy, virial and inside count.
+// kernel. Adds its force to (gx, gy, gz) and, with kEnergy, its energy, virial and inside count (a per-thread
+// 32-bit count: a thread visits far fewer than 2^32 row entries).
 template <bool kEnergy>
 __device__ __forceinline__ void float_pair(float dx, float dy, float dz, bool in, float r2, const FloatLJ& lj,
-                                           float& gx, float& gy, float& gz, float& ge, float& gw,
-                                           unsigned long long& ins) {
+                                           float& gx, float& gy, float& gz, float& ge, float& gw, unsigned& ins) {
     const float inv = rcp_approx(r2);
     const float sr2 = __fmul_rn(lj.sig2, inv);
     const float sr6 = __fmul_rn(__fmul_rn(sr2, sr2), sr2);
@@ -92,13 +92,63 @@ __device__ __forceinline__ void float_pair(float dx, float dy, float dz, bool in
     }
 }
 
-// Separation of a row entry's pair from the frames: (q_i - q_j) + image offset, and its float r^2
+// Separation of a row entry's pair from the frames: (q_i - q_j) + image offset, and its float r^2. x and y go
+// through one packed add of -q_j and one packed add of the offset (__fadd2_rn: the same two round-to-nearest
+// operations per component as the scalar sequence, so the same bits, in half the instructions).
 __device__ __forceinline__ float float_separation(const float4& qi, const float4& qj, const float4& o, float& dx,
                                                   float& dy, float& dz) {
-    dx = __fadd_rn(__fsub_rn(qi.x, qj.x), o.x);
-    dy = __fadd_rn(__fsub_rn(qi.y, qj.y), o.y);
+    const float2 d = __fadd2_rn(__fadd2_rn(make_float2(qi.x, qi.y), make_float2(-qj.x, -qj.y)), make_float2(o.x, o.y));
+    dx = d.x;
+    dy = d.y;
     dz = __fadd_rn(__fsub_rn(qi.z, qj.z), o.z);
     return fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
+}
+
+// Sums of one 8-entry group: force, energy, virial
+struct GroupSums {
+    float x = 0.f, y = 0.f, z = 0.f, e = 0.f, w = 0.f;
+};
+
+// One 8-entry group of a row (entries e0, e1 in order) through float_pair. sep(e, dx, dy, dz) returns the float
+// r^2 of entry e and its separation. The group runs branch-free with the float cutoff test; a pair in the
+// thin shell around r_c (about one group in a thousand has one) sends the whole group through
+// float_group_exact, the same sequence with the reference's exact test (exact(e)) deciding the shell pairs, so
+// the sums see the same operations in the same order either way. Adds the group's inside count to *ins.
+template <bool kEnergy, typename Sep, typename Exact>
+__device__ __noinline__ GroupSums float_group_exact(const uint4 e0, const uint4 e1, const FloatLJ lj, Sep sep,
+                                                    Exact exact, unsigned* gin) {
+    const uint32_t ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+    GroupSums g;
+    unsigned c = 0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        float dx, dy, dz;
+        const float r2 = sep(ent[u], dx, dy, dz);
+        bool in = r2 < lj.rc2;
+        if (fabsf(r2 - lj.rc2) < lj.band) in = exact(ent[u]);
+        float_pair<kEnergy>(dx, dy, dz, in, r2, lj, g.x, g.y, g.z, g.e, g.w, c);
+    }
+    *gin = c;
+    return g;
+}
+
+template <bool kEnergy, typename Sep, typename Exact>
+__device__ __forceinline__ GroupSums float_group(const uint4& e0, const uint4& e1, const FloatLJ& lj, Sep sep,
+                                                 Exact exact, unsigned& ins) {
+    const uint32_t ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+    GroupSums g;
+    unsigned c = 0;
+    bool shell = false;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        float dx, dy, dz;
+        const float r2 = sep(ent[u], dx, dy, dz);
+        shell |= fabsf(r2 - lj.rc2) < lj.band;
+        float_pair<kEnergy>(dx, dy, dz, r2 < lj.rc2, r2, lj, g.x, g.y, g.z, g.e, g.w, c);
+    }
+    if (shell) g = float_group_exact<kEnergy>(e0, e1, lj, sep, exact, &c);
+    ins += c;
+    return g;
 }
 
 // Per-particle accumulators of the float kernels: a group of 8 row entries goes into fixed point (FP32FX) or
@@ -219,43 +269,40 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_force_fp32_rows(const float
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     long long e_fx = 0, w_fx = 0, k_fx = 0;
-    unsigned long long ins = 0;
+    unsigned ins = 0;
     if (i < n) {
         const float4 qi = frames[i];
         const int2 c = counts[i];
         const int groups = (c.x + c.y + 7) >> 3;  // rows are padded with sentinels to a multiple of 8
         FloatAcc<kFixed, kEnergy> a;
+        // quad q of this particle's interleaved row is rq[32 q]; a group is two quads
+        const uint4* rq = reinterpret_cast<const uint4*>(rows) + static_cast<size_t>(i >> 5) * (cap >> 2) * 32 + (i & 31);
         uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
         if (kPrefetch && groups > 0) {
-            n0 = row_quad_stream(rows, i, 0, cap);
-            n1 = row_quad_stream(rows, i, 1, cap);
+            n0 = __ldcs(rq);
+            n1 = __ldcs(rq + 32);
         }
         for (int g = 0; g < groups; ++g) {
             uint4 e0, e1;
             if (kPrefetch) {
                 e0 = n0;
                 e1 = n1;
+                rq += 64;
                 if (g + 1 < groups) {
-                    n0 = row_quad_stream(rows, i, 2 * g + 2, cap);
-                    n1 = row_quad_stream(rows, i, 2 * g + 3, cap);
+                    n0 = __ldcs(rq);
+                    n1 = __ldcs(rq + 32);
                 }
             } else {
-                e0 = row_quad(rows, i, 2 * g, cap);
-                e1 = row_quad(rows, i, 2 * g + 1, cap);
+                e0 = rq[64 * g];
+                e1 = rq[64 * g + 32];
             }
-            const uint32_t ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
-            float gx = 0.f, gy = 0.f, gz = 0.f, ge = 0.f, gw = 0.f;
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const uint32_t e = ent[u];
-                const int j = static_cast<int>(e & kIndexMask);
-                float dx, dy, dz;
-                const float r2 = float_separation(qi, frames[j], s_off[e >> kCodeShift], dx, dy, dz);
-                bool in = r2 < lj.rc2;
-                if (fabsf(r2 - lj.rc2) < lj.band) in = exact_inside(pos[i], pos[j], box, lj.rc2d);
-                float_pair<kEnergy>(dx, dy, dz, in, r2, lj, gx, gy, gz, ge, gw, ins);
-            }
-            a.add_group(gx, gy, gz, ge, gw, e_fx, w_fx);
+            const GroupSums gs = float_group<kEnergy>(
+                e0, e1, lj,
+                [=](uint32_t e, float& dx, float& dy, float& dz) {
+                    return float_separation(qi, frames[e & kIndexMask], s_off[e >> kCodeShift], dx, dy, dz);
+                },
+                [=](uint32_t e) { return exact_inside(pos[i], pos[e & kIndexMask], box, lj.rc2d); }, ins);
+            a.add_group(gs.x, gs.y, gs.z, gs.e, gs.w, e_fx, w_fx);
         }
         k_fx = a.finish(i, n, force, kick);
     }
@@ -271,7 +318,7 @@ __global__ void k_force_fp32_small(const double4* __restrict__ pos, int n, Box b
                                    double* __restrict__ force, unsigned long long* __restrict__ acc, KickArgs kick) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     long long e_fx = 0, w_fx = 0, k_fx = 0;
-    unsigned long long ins = 0;
+    unsigned ins = 0;
     if (i < n) {
         const double4 pi = pos[i];
         const int2 c = counts[i];

@@ -61,7 +61,7 @@ __device__ __forceinline__ double fixed_separation(const int4& qi, const int4& q
 template <bool kEnergy>
 __device__ __forceinline__ void fx64_pair(double dx, double dy, double dz, bool in, double r2, const Fx64LJ& p,
                                           double& gx, double& gy, double& gz, double& ge, double& gw,
-                                          unsigned long long& ins) {
+                                          unsigned& ins) {
     double inv = static_cast<double>(rcp_approx(__double2float_rn(r2)));
     inv = __fma_rn(inv, __fma_rn(-r2, inv, 1.0), inv);
     inv = __fma_rn(inv, __fma_rn(-r2, inv, 1.0), inv);
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(128) k_force_fx64_rows(const int4* __restrict_
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     long long e_fx = 0, w_fx = 0, k_fx = 0;
-    unsigned long long ins = 0;
+    unsigned ins = 0;
     if (i < n) {
         const int4 qi = frames[i];
         const int2 c = counts[i];
@@ -132,7 +132,7 @@ __global__ void k_force_fx64_small(const double4* __restrict__ pos, int n, Box b
                                    double* __restrict__ force, unsigned long long* __restrict__ acc, KickArgs kick) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     long long e_fx = 0, w_fx = 0, k_fx = 0;
-    unsigned long long ins = 0;
+    unsigned ins = 0;
     if (i < n) {
         const double4 pi = pos[i];
         const int2 c = counts[i];

@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(kTileThreads) k_force_fp32_tile(
     cp_async_wait();
     __syncthreads();
     long long e_fx = 0, w_fx = 0, k_fx = 0;
-    unsigned long long ins = 0;
+    unsigned ins = 0;
     const int n = g.ncps;
     for (int i = t.home_begin + threadIdx.x; i < t.home_end; i += blockDim.x) {
         const int h = (cell_sorted[i] % n - t.z0 + n) % n;
@@ -300,21 +300,18 @@ __global__ void __launch_bounds__(kTileThreads) k_force_fp32_tile(
         for (int gi = 0; gi < groups; ++gi) {
             const uint4 e0 = row_quad(rows, i, 2 * gi, cap);
             const uint4 e1 = row_quad(rows, i, 2 * gi + 1, cap);
-            const uint32_t ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
-            float gx = 0.f, gy = 0.f, gz = 0.f, ge = 0.f, gw = 0.f;
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const uint32_t e = ent[u];
-                const float4 o = tab[e >> kCodeShift];
-                const unsigned slot = min(static_cast<unsigned>((e & kIndexMask) + __float_as_int(o.w)),
-                                          static_cast<unsigned>(sentinel_slot));
-                float dx, dy, dz;
-                const float r2 = float_separation(qi, s_q[slot], o, dx, dy, dz);
-                bool in = r2 < lj.rc2;
-                if (fabsf(r2 - lj.rc2) < lj.band) in = exact_inside(pos[i], pos[e & kIndexMask], g.box, lj.rc2d);
-                float_pair<kEnergy>(dx, dy, dz, in, r2, lj, gx, gy, gz, ge, gw, ins);
-            }
-            a.add_group(gx, gy, gz, ge, gw, e_fx, w_fx);
+            const float4* sq = s_q;
+            const Box box = g.box;
+            const GroupSums gs = float_group<kEnergy>(
+                e0, e1, lj,
+                [=](uint32_t e, float& dx, float& dy, float& dz) {
+                    const float4 o = tab[e >> kCodeShift];
+                    const unsigned slot = min(static_cast<unsigned>((e & kIndexMask) + __float_as_int(o.w)),
+                                              static_cast<unsigned>(sentinel_slot));
+                    return float_separation(qi, sq[slot], o, dx, dy, dz);
+                },
+                [=](uint32_t e) { return exact_inside(pos[i], pos[e & kIndexMask], box, lj.rc2d); }, ins);
+            a.add_group(gs.x, gs.y, gs.z, gs.e, gs.w, e_fx, w_fx);
         }
         k_fx += a.finish(i, n_atoms, force, kick);
     }
