@@ -195,29 +195,50 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
         int cnt = 0;
         // this particle's interleaved row: entry s at row[(s >> 2) * 128 + (s & 3)]
         uint32_t* row = rows + static_cast<size_t>(i >> 5) * (bp.cap >> 2) * 128 + (i & 31) * 4;
-        auto push = [&](int j, uint32_t code) {
-            if (cnt < bp.cap) row[(cnt >> 2) * 128 + (cnt & 3)] = static_cast<uint32_t>(j) | (code << kCodeShift);
-            ++cnt;
-        };
-        // qo = q_i + the cell's image offset, hoisted out of the candidate loop (the margin covers the rounding)
-        auto test = [&](int j, const float4& qj, const float4& qo) -> bool {
-            const float dx = qo.x - qj.x;
-            const float dy = qo.y - qj.y;
-            const float dz = qo.z - qj.z;
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            if (r2 < bp.rl2_lo) return true;
-            if (!(r2 <= bp.rl2_hi)) return false;
-            return exact_within(pi, pos[j], g.box, bp.rl2);  // thin shell: the reference's exact double test
+        // Candidates [u0, u1) of one staged cell, qo = q_i + the cell's image offset (the margin covers the
+        // rounding of the hoisted sum). The loop runs branch-free: a candidate below r_l^2 - margin is appended
+        // with a predicated store, one above r_l^2 + margin is dropped. If any candidate of the cell falls in
+        // the thin shell between, the cell is scanned again from its first slot with the reference's exact
+        // double test deciding the shell (rare), rewriting the same slots.
+        auto scan = [&](const float4* q, int gs, int u0, int u1, const float4& qo, uint32_t code) {
+            const int cnt0 = cnt;
+            bool shell = false;
+            for (int u = u0; u < u1; ++u) {
+                const float4 qj = q[u];
+                const float dx = qo.x - qj.x;
+                const float dy = qo.y - qj.y;
+                const float dz = qo.z - qj.z;
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const bool take = r2 < bp.rl2_lo;
+                shell |= !take && r2 <= bp.rl2_hi;
+                uint32_t* p = row + (cnt >> 2) * 128 + (cnt & 3);
+                if (take && cnt < bp.cap) *p = static_cast<uint32_t>(gs + u) | (code << kCodeShift);
+                cnt += take ? 1 : 0;
+            }
+            if (shell) {
+                cnt = cnt0;
+                for (int u = u0; u < u1; ++u) {
+                    const float4 qj = q[u];
+                    const float dx = qo.x - qj.x;
+                    const float dy = qo.y - qj.y;
+                    const float dz = qo.z - qj.z;
+                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    bool take = r2 < bp.rl2_lo;
+                    if (!take && r2 <= bp.rl2_hi) take = exact_within(pi, pos[gs + u], g.box, bp.rl2);
+                    if (take) {
+                        if (cnt < bp.cap) row[(cnt >> 2) * 128 + (cnt & 3)] = static_cast<uint32_t>(gs + u) | (code << kCodeShift);
+                        ++cnt;
+                    }
+                }
+            }
         };
         // own pairs: 27 cells in (dx, dy, dz) order, increasing j inside each (src/CellList.cpp:55-83)
         for (uint32_t code = 0; code < 27; ++code) {
             const int sc = staged_cell(static_cast<int>(code), h, span);
             const float4 o = offs.off[code];
             const float4 qo = make_float4(qi.x + o.x, qi.y + o.y, qi.z + o.z, 0.0f);
-            const int gs = t.gstart[sc], cc = t.count[sc];
-            const float4* q = s_q + t.off[sc];
-            for (int u = max(0, i + 1 - gs); u < cc; ++u)
-                if (test(gs + u, q[u], qo)) push(gs + u, code);
+            const int gs = t.gstart[sc];
+            scan(s_q + t.off[sc], gs, max(0, i + 1 - gs), t.count[sc], qo, code);
         }
         const int own = cnt;
         // the j < i that list i, increasing j: cells in increasing cell id
@@ -238,11 +259,8 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
                     const int sc = staged_cell(static_cast<int>(code), h, span);
                     const float4 o = offs.off[code];
                     const float4 qo = make_float4(qi.x + o.x, qi.y + o.y, qi.z + o.z, 0.0f);
-                    const int gs = t.gstart[sc], cc = t.count[sc];
-                    const float4* q = s_q + t.off[sc];
-                    const int ue = min(cc, i - gs);
-                    for (int u = 0; u < ue; ++u)
-                        if (test(gs + u, q[u], qo)) push(gs + u, code);
+                    const int gs = t.gstart[sc];
+                    scan(s_q + t.off[sc], gs, 0, min(t.count[sc], i - gs), qo, code);
                 }
         counts[i] = make_int2(own, cnt - own);
         const int padded = (cnt + 7) & ~7;
