@@ -19,6 +19,7 @@
 #include "md_cells.cuh"
 #include "md_common.cuh"
 #include "md_fp32.cuh"
+#include "md_tiles.cuh"
 #include "md_fp64.cuh"
 #include "md_nlist.cuh"
 
@@ -382,12 +383,11 @@ __global__ void __launch_bounds__(kTile)
             const float4 qi = frames[a];
             const float cellf = static_cast<float>(d.cell);
             const int* st = start + d.cell_off + r;
-            // qo = q_i + the cell's image offset, computed once per candidate cell (the margin covers the rounding)
-            auto take = [&](int j, uint32_t code, const float4& qo) {
-                const float4 qj = frames[j];
-                const float dx = qo.x - qj.x, dy = qo.y - qj.y, dz = qo.z - qj.z;
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                if (r2 < bp.lo || (r2 <= bp.hi && within_rl(pi, pos[j], d.box, bp.rl2))) push(j, code);
+            uint32_t* row = rows + row_index(a, 0, bp.cap);
+            // candidates [j0, j1) of one cell (scan_cell: branch-free float screen, exact shell re-scan);
+            // qo = q_i + the cell's image offset, computed once per candidate cell
+            auto take = [&](int j0, int j1, uint32_t code, const float4& qo) {
+                scan_cell(frames + j0, j0, 0, j1 - j0, qo, code, bp.lo, bp.hi, bp.rl2, bp.cap, pi, pos, d.box, row, cnt);
             };
             auto shifted = [&](uint32_t code) {
                 const float4 o = code_offset(static_cast<int>(code), cellf);
@@ -404,8 +404,8 @@ __global__ void __launch_bounds__(kTile)
                         const int cell = (x * nc + y) * nc + (cz + dz + nc) % nc;
                         const uint32_t code = (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
                         const int e = st[cell + 1];
-                        const float4 qo = shifted(code);
-                        for (int j = st[cell] > a + 1 ? st[cell] : a + 1; j < e; ++j) take(j, code, qo);
+                        const int j0 = st[cell] > a + 1 ? st[cell] : a + 1;
+                        if (j0 < e) take(j0, e, code, shifted(code));
                     }
                 }
             }
@@ -422,8 +422,7 @@ __global__ void __launch_bounds__(kTile)
                         const int cell = (x * nc + y) * nc + (cz + oz[q] + nc) % nc;
                         const uint32_t code = (ox[u] + 1) * 9 + (oy[v] + 1) * 3 + (oz[q] + 1);
                         const int e = st[cell + 1] < a ? st[cell + 1] : a;
-                        const float4 qo = shifted(code);
-                        for (int j = st[cell]; j < e; ++j) take(j, code, qo);
+                        if (st[cell] < e) take(st[cell], e, code, shifted(code));
                     }
                 }
             }

@@ -171,6 +171,49 @@ __device__ __noinline__ bool exact_within(const double4& pi, const double4& pj, 
     return norm2(ex, ey, ez) < rl2;
 }
 
+// Appends to a row the candidates u in [u0, u1) of one cell that are within r_l of particle i: candidate u has
+// the float frame q[u] and the index jbase + u, qo = q_i + the cell's image offset (the margin covers the
+// rounding of that hoisted sum), row is particle i's interleaved row (entry s at row[(s >> 2) * 128 + (s & 3)])
+// and cnt its length. The loop runs branch-free: a candidate whose float r^2 is below lo = r_l^2 - margin is
+// appended with a predicated store, one above hi = r_l^2 + margin is dropped. If any candidate of the cell falls
+// in the thin shell between, the cell is scanned again from its first slot with the reference's exact double
+// test (src/NeighbourList.cpp:38-52) deciding the shell, rewriting the same slots. Entries past cap are counted
+// and not written.
+__device__ __forceinline__ void scan_cell(const float4* q, int jbase, int u0, int u1, const float4& qo, uint32_t code,
+                                          float lo, float hi, double rl2, int cap, const double4& pi,
+                                          const double4* __restrict__ pos, const Box& box, uint32_t* row, int& cnt) {
+    const int cnt0 = cnt;
+    bool shell = false;
+    for (int u = u0; u < u1; ++u) {
+        const float4 qj = q[u];
+        const float dx = qo.x - qj.x;
+        const float dy = qo.y - qj.y;
+        const float dz = qo.z - qj.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const bool take = r2 < lo;
+        shell |= !take && r2 <= hi;
+        uint32_t* p = row + (cnt >> 2) * 128 + (cnt & 3);
+        if (take && cnt < cap) *p = static_cast<uint32_t>(jbase + u) | (code << kCodeShift);
+        cnt += take ? 1 : 0;
+    }
+    if (shell) {
+        cnt = cnt0;
+        for (int u = u0; u < u1; ++u) {
+            const float4 qj = q[u];
+            const float dx = qo.x - qj.x;
+            const float dy = qo.y - qj.y;
+            const float dz = qo.z - qj.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            bool take = r2 < lo;
+            if (!take && r2 <= hi) take = exact_within(pi, pos[jbase + u], box, rl2);
+            if (take) {
+                if (cnt < cap) row[(cnt >> 2) * 128 + (cnt & 3)] = static_cast<uint32_t>(jbase + u) | (code << kCodeShift);
+                ++cnt;
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
     const float4* __restrict__ frames, const double4* __restrict__ pos, const int* __restrict__ cell_start,
     const int* __restrict__ cell_sorted, TileGeom g, BuildParams bp, CellOffsets offs, uint32_t* __restrict__ rows,
@@ -195,42 +238,8 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
         int cnt = 0;
         // this particle's interleaved row: entry s at row[(s >> 2) * 128 + (s & 3)]
         uint32_t* row = rows + static_cast<size_t>(i >> 5) * (bp.cap >> 2) * 128 + (i & 31) * 4;
-        // Candidates [u0, u1) of one staged cell, qo = q_i + the cell's image offset (the margin covers the
-        // rounding of the hoisted sum). The loop runs branch-free: a candidate below r_l^2 - margin is appended
-        // with a predicated store, one above r_l^2 + margin is dropped. If any candidate of the cell falls in
-        // the thin shell between, the cell is scanned again from its first slot with the reference's exact
-        // double test deciding the shell (rare), rewriting the same slots.
         auto scan = [&](const float4* q, int gs, int u0, int u1, const float4& qo, uint32_t code) {
-            const int cnt0 = cnt;
-            bool shell = false;
-            for (int u = u0; u < u1; ++u) {
-                const float4 qj = q[u];
-                const float dx = qo.x - qj.x;
-                const float dy = qo.y - qj.y;
-                const float dz = qo.z - qj.z;
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const bool take = r2 < bp.rl2_lo;
-                shell |= !take && r2 <= bp.rl2_hi;
-                uint32_t* p = row + (cnt >> 2) * 128 + (cnt & 3);
-                if (take && cnt < bp.cap) *p = static_cast<uint32_t>(gs + u) | (code << kCodeShift);
-                cnt += take ? 1 : 0;
-            }
-            if (shell) {
-                cnt = cnt0;
-                for (int u = u0; u < u1; ++u) {
-                    const float4 qj = q[u];
-                    const float dx = qo.x - qj.x;
-                    const float dy = qo.y - qj.y;
-                    const float dz = qo.z - qj.z;
-                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                    bool take = r2 < bp.rl2_lo;
-                    if (!take && r2 <= bp.rl2_hi) take = exact_within(pi, pos[gs + u], g.box, bp.rl2);
-                    if (take) {
-                        if (cnt < bp.cap) row[(cnt >> 2) * 128 + (cnt & 3)] = static_cast<uint32_t>(gs + u) | (code << kCodeShift);
-                        ++cnt;
-                    }
-                }
-            }
+            scan_cell(q, gs, u0, u1, qo, code, bp.rl2_lo, bp.rl2_hi, bp.rl2, bp.cap, pi, pos, g.box, row, cnt);
         };
         // own pairs: 27 cells in (dx, dy, dz) order, increasing j inside each (src/CellList.cpp:55-83)
         for (uint32_t code = 0; code < 27; ++code) {
