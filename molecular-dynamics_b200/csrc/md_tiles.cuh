@@ -184,17 +184,33 @@ __device__ __forceinline__ void scan_cell(const float4* q, int jbase, int u0, in
                                           const double4* __restrict__ pos, const Box& box, uint32_t* row, int& cnt) {
     const int cnt0 = cnt;
     bool shell = false;
-    for (int u = u0; u < u1; ++u) {
-        const float4 qj = q[u];
-        const float dx = qo.x - qj.x;
-        const float dy = qo.y - qj.y;
-        const float dz = qo.z - qj.z;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const bool take = r2 < lo;
-        shell |= !take && r2 <= hi;
-        uint32_t* p = row + (cnt >> 2) * 128 + (cnt & 3);
-        if (take && cnt < cap) *p = static_cast<uint32_t>(jbase + u) | (code << kCodeShift);
-        cnt += take ? 1 : 0;
+    const uint32_t vbase = static_cast<uint32_t>(jbase) | (code << kCodeShift);  // entry of candidate u: vbase + u
+    if (cnt + (u1 - u0) <= cap) {  // every candidate fits: no capacity test per candidate
+        for (int u = u0; u < u1; ++u) {
+            const float4 qj = q[u];
+            const float dx = qo.x - qj.x;
+            const float dy = qo.y - qj.y;
+            const float dz = qo.z - qj.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const bool take = r2 < lo;
+            shell |= !take && r2 <= hi;
+            uint32_t* p = row + (cnt + 31 * (cnt & ~3));  // (cnt >> 2) * 128 + (cnt & 3)
+            asm volatile("{\n\t.reg .pred t;\n\tsetp.ne.u32 t, %2, 0;\n\t@t st.global.u32 [%0], %1;\n\t}"
+                         :: "l"(p), "r"(vbase + static_cast<uint32_t>(u)), "r"(static_cast<unsigned>(take)) : "memory");
+            cnt += take ? 1 : 0;
+        }
+    } else {
+        for (int u = u0; u < u1; ++u) {
+            const float4 qj = q[u];
+            const float dx = qo.x - qj.x;
+            const float dy = qo.y - qj.y;
+            const float dz = qo.z - qj.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const bool take = r2 < lo;
+            shell |= !take && r2 <= hi;
+            if (take && cnt < cap) row[(cnt >> 2) * 128 + (cnt & 3)] = vbase + static_cast<uint32_t>(u);
+            cnt += take ? 1 : 0;
+        }
     }
     if (shell) {
         cnt = cnt0;
