@@ -79,6 +79,12 @@ struct DevBuf {
     }
 };
 
+template <typename T>
+void swap_buffers(DevBuf<T>& a, DevBuf<T>& b) {
+    std::swap(a.p, b.p);
+    std::swap(a.count, b.count);
+}
+
 inline unsigned blocks_for(long long n, int threads) {
     return static_cast<unsigned>((n + threads - 1) / threads);
 }
@@ -121,6 +127,16 @@ struct md_system {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t frame_ready = nullptr;
 };
+
+// After k_permute: the permuted arrays become the system's, the old ones its reorder buffers. No device
+// pointer of a system outlives a call, so the swap is invisible outside the library.
+inline void swap_reordered(md_system* s) {
+    swap_buffers(s->pos, s->pos2);
+    swap_buffers(s->vel, s->vel2);
+    swap_buffers(s->force, s->force2);
+    swap_buffers(s->mass, s->mass2);
+    swap_buffers(s->ids, s->ids2);
+}
 
 struct CellGrid {
     int ncps = 0, ncells = 0;
@@ -339,7 +355,7 @@ unsigned tile_blocks(const TileGeom& g) { return static_cast<unsigned>(g.ncps) *
 
 // NeighbourList::build (src/NeighbourList.cpp:55-134) on the device. The reference builds the cell list,
 // reorders the system, and builds the cell list again; the second build only recomputes the cells of the
-// already sorted particles (same positions, identity order), which k_permute_commit writes directly.
+// already sorted particles (same positions, identity order), which k_permute writes directly.
 md_status nlist_build(md_nlist* nl, md_system* s) {
     if (2.0 * nl->rl > s->box.L) return fail(MD_ERR_LIST_RADIUS, "Cutoff + skin must be less than half the box length");
     const int n = static_cast<int>(s->n);
@@ -355,12 +371,9 @@ md_status nlist_build(md_nlist* nl, md_system* s) {
     if (n > 0) {
         k_permute<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(
             nl->grid.order.p, n, s->pos.p, s->vel.p, s->force.p, s->mass.p, s->ids.p, s->pos2.p, s->vel2.p,
-            s->force2.p, s->mass2.p, s->ids2.p);
+            s->force2.p, s->mass2.p, s->ids2.p, nl->grid.cell_of.p, nl->cell_sorted.p, nl->ref_pos.p);
         MD_CHECK_LAUNCH();
-        k_permute_commit<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(
-            n, nl->grid.order.p, nl->grid.cell_of.p, s->pos2.p, s->vel2.p, s->force2.p, s->mass2.p, s->ids2.p,
-            s->pos.p, s->vel.p, s->force.p, s->mass.p, s->ids.p, nl->cell_sorted.p, nl->ref_pos.p);
-        MD_CHECK_LAUNCH();
+        swap_reordered(s);
     }
     s->layout++;
     nl->use_cells = nl->grid.ncps >= 3;  // src/NeighbourList.cpp:69
@@ -805,12 +818,9 @@ md_status md_system_reorder(md_system* s, const uint64_t* order) {
     MD_CUDA(s->ids2.reserve(n));
     k_permute<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(d.p, n, s->pos.p, s->vel.p, s->force.p, s->mass.p,
                                                                    s->ids.p, s->pos2.p, s->vel2.p, s->force2.p,
-                                                                   s->mass2.p, s->ids2.p);
+                                                                   s->mass2.p, s->ids2.p, nullptr, nullptr, nullptr);
     MD_CHECK_LAUNCH();
-    k_permute_commit<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(
-        n, d.p, nullptr, s->pos2.p, s->vel2.p, s->force2.p, s->mass2.p, s->ids2.p, s->pos.p, s->vel.p, s->force.p,
-        s->mass.p, s->ids.p, nullptr, nullptr);
-    MD_CHECK_LAUNCH();
+    swap_reordered(s);
     s->layout++;
     return sync(s);
 }

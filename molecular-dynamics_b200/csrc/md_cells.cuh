@@ -41,7 +41,8 @@ __global__ void k_cell_scatter(const int* __restrict__ cell_of, int n, const int
 
 // One warp per cell: each particle's rank in its cell is the number of smaller indices in the bucket, so
 // order[] lists every cell's particles in increasing index, as the reference's serial scatter does
-// (src/CellList.cpp:48-51).
+// (src/CellList.cpp:48-51). A cell of up to 32 particles is ranked from registers (one index per lane, compared
+// through shuffles); larger cells compare against the bucket in memory.
 // max_occ receives the largest cell occupancy (it sizes the shared-memory tiles).
 __global__ void k_cell_rank(const int* __restrict__ start, int ncells, const uint32_t* __restrict__ bucket,
                             uint32_t* __restrict__ order, int* __restrict__ max_occ) {
@@ -51,6 +52,13 @@ __global__ void k_cell_rank(const int* __restrict__ start, int ncells, const uin
     const int s = start[warp];
     const int m = start[warp + 1] - s;
     if (lane == 0) atomicMax(max_occ, m);
+    if (m <= 32) {
+        const uint32_t v = lane < m ? bucket[s + lane] : 0xffffffffu;
+        int rank = 0;
+        for (int f = 0; f < m; ++f) rank += __shfl_sync(0xffffffffu, v, f) < v;
+        if (lane < m) order[s + rank] = v;
+        return;
+    }
     for (int e = lane; e < m; e += 32) {
         const uint32_t v = bucket[s + e];
         int rank = 0;
@@ -59,16 +67,20 @@ __global__ void k_cell_rank(const int* __restrict__ start, int ncells, const uin
     }
 }
 
-// new[k] = old[order[k]] for every per-particle array (src/System.cpp:42-64)
+// new[k] = old[order[k]] for every per-particle array (src/System.cpp:42-64); the caller swaps the buffers.
+// With cell_of_old, also the list's per-particle cell (cell_of of the sorted order) and its reference positions
+// (src/NeighbourList.cpp:129-132).
 __global__ void k_permute(const uint32_t* __restrict__ order, int n, const double4* __restrict__ pos,
                           const double* __restrict__ vel, const double* __restrict__ force,
                           const double* __restrict__ mass, const uint64_t* __restrict__ ids,
                           double4* __restrict__ pos2, double* __restrict__ vel2, double* __restrict__ force2,
-                          double* __restrict__ mass2, uint64_t* __restrict__ ids2) {
+                          double* __restrict__ mass2, uint64_t* __restrict__ ids2, const int* __restrict__ cell_of_old,
+                          int* __restrict__ cell_sorted, double4* __restrict__ ref_pos) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const uint32_t o = order[k];
-    pos2[k] = pos[o];
+    const double4 p = pos[o];
+    pos2[k] = p;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         vel2[static_cast<size_t>(c) * n + k] = vel[static_cast<size_t>(c) * n + o];
@@ -76,30 +88,10 @@ __global__ void k_permute(const uint32_t* __restrict__ order, int n, const doubl
     }
     mass2[k] = mass[o];
     ids2[k] = ids[o];
-}
-
-// Copy the permuted arrays back, and give the list its per-particle cell (cell_of of the sorted order) and
-// its reference positions (src/NeighbourList.cpp:129-132).
-__global__ void k_permute_commit(int n, const uint32_t* __restrict__ order, const int* __restrict__ cell_of_old,
-                                 const double4* __restrict__ pos2, const double* __restrict__ vel2,
-                                 const double* __restrict__ force2, const double* __restrict__ mass2,
-                                 const uint64_t* __restrict__ ids2, double4* __restrict__ pos,
-                                 double* __restrict__ vel, double* __restrict__ force, double* __restrict__ mass,
-                                 uint64_t* __restrict__ ids, int* __restrict__ cell_sorted,
-                                 double4* __restrict__ ref_pos) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const double4 p = pos2[k];
-    pos[k] = p;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        vel[static_cast<size_t>(c) * n + k] = vel2[static_cast<size_t>(c) * n + k];
-        force[static_cast<size_t>(c) * n + k] = force2[static_cast<size_t>(c) * n + k];
+    if (cell_of_old) {
+        cell_sorted[k] = cell_of_old[o];
+        ref_pos[k] = p;
     }
-    mass[k] = mass2[k];
-    ids[k] = ids2[k];
-    if (cell_sorted) cell_sorted[k] = cell_of_old[order[k]];
-    if (ref_pos) ref_pos[k] = p;
 }
 
 // out[6 id + k] = (x, y, z, vx, vy, vz)[k] of the particle whose id is `id` (ids are a permutation of 0..n-1;
