@@ -189,6 +189,7 @@ struct md_forcefield {
     double virial = 0.0, inside = 0.0;
     int device = -1;
     DevBuf<double2> eblocks;
+    DevBuf<double2> pair_ew;  // FP64 energies: (pairEnergy, pairVirial) of every own pair, in pair order
     DevBuf<double> out;  // [0] pe, [1] virial, [2] inside
     DevBuf<unsigned long long> inside_count;
     DevBuf<long long> fx_acc;  // fixed-point accumulators of the float kernels: pe, virial
@@ -543,8 +544,11 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
     MD_CUDA(cudaMemsetAsync(ff->inside_count.p, 0, sizeof(unsigned long long), s->stream));
     if (ff->precision == MD_PREC_FP64) {
         if (n > 0) {
-            // variant 0: global gathers; variant 1: shared-memory tile (both bit-identical)
-            auto launch = [&](int variant, bool kick) -> md_status {
+            // variant 0: global gathers; variant 1: shared-memory tile (both bit-identical). With want_energy the
+            // kernel also stores every own pair's (E, W) in pair order for the blocked sums below.
+            const long long pairs = static_cast<long long>(nl->pairs);
+            if (want_energy) MD_CUDA(ff->pair_ew.reserve(static_cast<size_t>(pairs)));
+            auto launch = [&](int variant, bool kick, double2* ew) -> md_status {
                 if (variant == 1) {
                     const TileGeom& tg = nl->tiles_geom;
                     const size_t smem = sizeof(double4) * tg.max_staged;
@@ -554,31 +558,27 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
                     const KickArgs ka{kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
                     k_force_fp64_tile<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
                         s->pos.p, n, nl->grid.start.p, nl->cell_sorted.p, tg, ff->lj, nl->rows.p, nl->cap,
-                        nl->counts.p, s->force.p, ff->inside_count.p, ka);
+                        nl->counts.p, s->force.p, ff->inside_count.p, ka, nl->half_off.p, ew);
                 } else {
                     k_force_fp64<<<blocks_for(n, 128), 128, 0, s->stream>>>(
                         s->pos.p, n, s->box, ff->lj, nl->rows.p, nl->cap, nl->counts.p, s->force.p, ff->inside_count.p,
-                        kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt);
+                        kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt, nl->half_off.p, ew);
                 }
                 MD_CHECK_LAUNCH();
                 return MD_OK;
             };
-            MD_TRY(choose_variant(s, nl, MD_PREC_FP64, [&](int v) { return launch(v, false); }));
+            MD_TRY(choose_variant(s, nl, MD_PREC_FP64, [&](int v) { return launch(v, false, nullptr); }));
             MD_CUDA(cudaMemsetAsync(ff->inside_count.p, 0, sizeof(unsigned long long), s->stream));
             MD_TRY(profile_mark(s));
-            MD_TRY(launch(nl->variant[MD_PREC_FP64], kick_dt > 0.0));
+            MD_TRY(launch(nl->variant[MD_PREC_FP64], kick_dt > 0.0, want_energy ? ff->pair_ew.p : nullptr));
             MD_TRY(profile_mark(s));
         }
         if (want_energy) {
-            const long long pairs = static_cast<long long>(nl->pairs);
+            const long long pairs = n > 0 ? static_cast<long long>(nl->pairs) : 0;
             const int nb = static_cast<int>((pairs + kChunk - 1) / kChunk);
             if (nb > 0) {
                 MD_CUDA(ff->eblocks.reserve(nb));
-                const size_t smem = kEnergyWarps * kChunk * sizeof(double2);
-                MD_CUDA(cudaFuncSetAttribute(k_energy_blocks_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem)));
-                k_energy_blocks_fp64<<<blocks_for(nb, kEnergyWarps), kEnergyWarps * 32, smem, s->stream>>>(
-                    s->pos.p, n, s->box, ff->lj, nl->rows.p, nl->cap, nl->half_off.p, pairs, ff->eblocks.p, nb);
+                k_pair_block_sums<<<blocks_for(nb, 128), 128, 0, s->stream>>>(ff->pair_ew.p, pairs, ff->eblocks.p, nb);
                 MD_CHECK_LAUNCH();
                 k_sum_blocks<<<1, 32, 0, s->stream>>>(ff->eblocks.p, nb, ff->out.p);
                 MD_CHECK_LAUNCH();

@@ -779,7 +779,10 @@ __global__ void __launch_bounds__(kRepScanThreads) k_b_pair_items(int R, const i
     if (threadIdx.x == 0) item_off[R] = s_carry;
 }
 
-// k_energy_blocks_fp64 per replica: each warp takes 1024-pair blocks (items) of all replicas in turn
+// Per replica: energy and virial of each 1024-pair block of the half list in the reference's pair order, summed
+// from 0.0 one after another (deterministicSum's inner loop, include/Parallel.hpp:43-46; pairEnergy/pairVirial
+// of src/Forcefield.cpp:288-296). Each warp takes blocks (items) of all replicas in turn: the lanes evaluate the
+// block's pairs into shared memory, lane 0 adds them in order.
 __global__ void k_b_energy_blocks(const BRep* __restrict__ reps, int R, const int* __restrict__ item_off,
                                   const int* __restrict__ pairs, const int* __restrict__ half_off,
                                   const double4* __restrict__ pos, LJ lj, const uint32_t* __restrict__ rows, int cap,

@@ -14,15 +14,23 @@ namespace md {
 // index. Pairs outside the cutoff contribute an exact zero in the reference and are skipped here. The
 // inside-cutoff count is the number of own pairs with r^2 < r_c^2 (a sum of whole numbers, exact).
 // With kick_vel set it also applies the closing half kick, v += (half_dt F) / m, with k_kick's sequence.
+// With pair_ew set, own pair s of particle i also stores (pairEnergy, pairVirial) at pair_ew[half_off[i] + s]:
+// E and (F/r) r^2 inside the cutoff, (0, 0) outside (src/Forcefield.cpp:288-296), for k_pair_block_sums.
+__device__ __forceinline__ void store_pair_ew(double2* pair_ew, long long k, bool in, double f, double e, double r2) {
+    pair_ew[k] = in ? make_double2(e, dmul(f, r2)) : make_double2(0.0, 0.0);
+}
+
 __global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ lj, const uint32_t* __restrict__ rows,
                              int cap, const int2* __restrict__ counts, double* __restrict__ force,
                              unsigned long long* __restrict__ inside, double* __restrict__ kick_vel,
-                             const double* __restrict__ mass, double half_dt) {
+                             const double* __restrict__ mass, double half_dt, const long long* __restrict__ half_off,
+                             double2* __restrict__ pair_ew) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long ins = 0;
     if (i < n) {
         const double4 pi = pos[i];
         const int2 c = counts[i];
+        const long long pb = pair_ew ? half_off[i] : 0;
         double fx = 0.0, fy = 0.0, fz = 0.0;
         for (int s = 0; s < c.x; ++s) {
             const double4 pj = pos[rows[row_index(i, s, cap)] & kIndexMask];
@@ -30,9 +38,13 @@ __global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ
             const double dy = min_image(dsub(pi.y, pj.y), box);
             const double dz = min_image(dsub(pi.z, pj.z), box);
             const double r2 = norm2(dx, dy, dz);
-            if (!(r2 < lj.rc2)) continue;
+            if (!(r2 < lj.rc2)) {
+                if (pair_ew) store_pair_ew(pair_ew, pb + s, false, 0.0, 0.0, r2);
+                continue;
+            }
             double f, e;
             pair_terms(r2, lj, f, e);
+            if (pair_ew) store_pair_ew(pair_ew, pb + s, true, f, e, r2);
             fx = dadd(fx, dmul(f, dx));
             fy = dadd(fy, dmul(f, dy));
             fz = dadd(fz, dmul(f, dz));
@@ -63,78 +75,57 @@ __global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ
     if ((threadIdx.x & 31) == 0 && ins) atomicAdd(inside, ins);
 }
 
-// Energy and virial of pairs [k0, k1) of the half list in the reference's pair order, summed from 0.0 one
-// after another (the inner loop of deterministicSum, include/Parallel.hpp:43-46): pairEnergy[k] = E when
-// r^2 < r_c^2 else 0, pairVirial[k] = (F/r) r^2 likewise (src/Forcefield.cpp:288-296). One warp per
-// 1024-pair block; lanes evaluate pairs into shared memory, lane 0 sums them in order.
-constexpr int kEnergyWarps = 4;
-__global__ void k_energy_blocks_fp64(const double4* __restrict__ pos, int n, Box box, LJ lj,
-                                     const uint32_t* __restrict__ rows, int cap,
-                                     const long long* __restrict__ half_off, long long pairs,
-                                     double2* __restrict__ block_sums, int nblocks) {
-    extern __shared__ double2 sm_ew[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int blk = blockIdx.x * kEnergyWarps + warp;
-    if (blk >= nblocks) return;
-    double2* ew = sm_ew + warp * kChunk;
-    const long long k0 = static_cast<long long>(blk) * kChunk;
-    const long long k1 = k0 + kChunk < pairs ? k0 + kChunk : pairs;
-    // first particle whose pairs reach k0: the last i with half_off[i] <= k0
-    int i = 0;
-    if (lane == 0) {
-        int lo = 0, hi = n;  // half_off[lo] <= k0 < half_off[hi]
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (half_off[mid] <= k0) lo = mid; else hi = mid;
-        }
-        i = lo;
+constexpr int kEnergyWarps = 4;  // warps per block of the blocked kinetic-energy sums
+
+// The inner loop of deterministicSum (include/Parallel.hpp:43-46) over the (pairEnergy, pairVirial) array the
+// force kernel stored: block b sums pairs [1024 b, 1024 b + 1024) from 0.0 one after another. One lane per
+// block, so a warp advances 32 blocks' ordered sums together.
+__global__ void k_pair_block_sums(const double2* __restrict__ pair_ew, long long pairs, double2* __restrict__ block_sums,
+                                  int nblocks) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblocks) return;
+    const long long k0 = static_cast<long long>(b) * kChunk;
+    const int m = static_cast<int>(pairs - k0 < kChunk ? pairs - k0 : kChunk);
+    const double2* v = pair_ew + k0;
+    double se = 0.0, sw = 0.0;
+    for (int t = 0; t < m; ++t) {
+        const double2 x = v[t];
+        se = dadd(se, x.x);
+        sw = dadd(sw, x.y);
     }
-    i = __shfl_sync(0xffffffffu, i, 0);
-    for (; i < n && half_off[i] < k1; ++i) {
-        const long long b = half_off[i];
-        const long long kb = b > k0 ? b : k0;
-        const long long ke = half_off[i + 1] < k1 ? half_off[i + 1] : k1;
-        const double4 pi = pos[i];
-        for (long long k = kb + lane; k < ke; k += 32) {
-            const double4 pj = pos[rows[row_index(i, static_cast<int>(k - b), cap)] & kIndexMask];
-            const double dx = min_image(dsub(pi.x, pj.x), box);
-            const double dy = min_image(dsub(pi.y, pj.y), box);
-            const double dz = min_image(dsub(pi.z, pj.z), box);
-            const double r2 = norm2(dx, dy, dz);
-            double f, e;
-            pair_terms(r2, lj, f, e);
-            const bool in = r2 < lj.rc2;
-            f = in ? f : 0.0;
-            ew[k - k0] = make_double2(in ? e : 0.0, dmul(f, r2));
-        }
-    }
-    __syncwarp();
-    if (lane == 0) {
-        double se = 0.0, sw = 0.0;
-        const int m = static_cast<int>(k1 - k0);
-        for (int t = 0; t < m; ++t) {
-            const double2 v = ew[t];
-            se = dadd(se, v.x);
-            sw = dadd(sw, v.y);
-        }
-        block_sums[blk] = make_double2(se, sw);
-    }
+    block_sums[b] = make_double2(se, sw);
 }
 
 // The outer loop of deterministicSum (include/Parallel.hpp:52-56): block sums added in order from 0.0.
-// One warp; lanes stage 32 values at a time, lane 0 adds them one after another.
+// One warp: the lanes stage 256 values at a time in shared memory (the next chunk's loads in flight while
+// lane 0 adds the current one, one value after another).
 __global__ void k_sum_blocks(const double2* __restrict__ block_sums, int nblocks, double* __restrict__ out) {
+    constexpr int kStage = 256;
+    __shared__ double2 stage[kStage];
     const int lane = threadIdx.x & 31;
+    double2 next[kStage / 32];
+    auto fetch = [&](int c) {
+#pragma unroll
+        for (int q = 0; q < kStage / 32; ++q) {
+            const int k = c * kStage + q * 32 + lane;
+            next[q] = k < nblocks ? block_sums[k] : make_double2(0.0, 0.0);
+        }
+    };
     double se = 0.0, sw = 0.0;
-    for (int b0 = 0; b0 < nblocks; b0 += 32) {
-        const double2 v = b0 + lane < nblocks ? block_sums[b0 + lane] : make_double2(0.0, 0.0);
-        const int m = nblocks - b0 < 32 ? nblocks - b0 : 32;
-        for (int t = 0; t < m; ++t) {
-            const double x = __shfl_sync(0xffffffffu, v.x, t);
-            const double y = __shfl_sync(0xffffffffu, v.y, t);
-            if (lane == 0) {
-                se = dadd(se, x);
-                sw = dadd(sw, y);
+    const int chunks = (nblocks + kStage - 1) / kStage;
+    if (chunks > 0) fetch(0);
+    for (int c = 0; c < chunks; ++c) {
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < kStage / 32; ++q) stage[q * 32 + lane] = next[q];
+        __syncwarp();
+        if (c + 1 < chunks) fetch(c + 1);
+        if (lane == 0) {
+            const int m = nblocks - c * kStage < kStage ? nblocks - c * kStage : kStage;
+            for (int t = 0; t < m; ++t) {
+                const double2 x = stage[t];
+                se = dadd(se, x.x);
+                sw = dadd(sw, x.y);
             }
         }
     }
