@@ -141,7 +141,6 @@ inline void swap_reordered(md_system* s) {
 struct CellGrid {
     int ncps = 0, ncells = 0;
     DevBuf<int> cell_of, count, start, cursor;
-    DevBuf<int> max_occ;  // largest cell occupancy of the last sort
     DevBuf<uint32_t> bucket, order;
     DevBuf<long long> tiles;
 };
@@ -285,8 +284,6 @@ md_status cell_sort(CellGrid& g, md_system* s, double min_size) {
     MD_CUDA(g.tiles.reserve(scan_tiles_needed(g.ncells)));
     MD_CUDA(cudaMemsetAsync(g.count.p, 0, sizeof(int) * g.ncells, s->stream));
     MD_CUDA(cudaMemsetAsync(g.cursor.p, 0, sizeof(int) * g.ncells, s->stream));
-    MD_CUDA(g.max_occ.reserve(1));
-    MD_CUDA(cudaMemsetAsync(g.max_occ.p, 0, sizeof(int), s->stream));
     if (n > 0) {
         k_cell_assign<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(s->pos.p, n, inv_cell, g.ncps, g.cell_of.p,
                                                                            g.count.p);
@@ -299,7 +296,7 @@ md_status cell_sort(CellGrid& g, md_system* s, double min_size) {
                                                                             g.bucket.p);
         MD_CHECK_LAUNCH();
         k_cell_rank<<<blocks_for(static_cast<long long>(g.ncells) * 32, kThreads), kThreads, 0, s->stream>>>(
-            g.start.p, g.ncells, g.bucket.p, g.order.p, g.max_occ.p);
+            g.start.p, g.ncells, g.bucket.p, g.order.p);
         MD_CHECK_LAUNCH();
     }
     return MD_OK;

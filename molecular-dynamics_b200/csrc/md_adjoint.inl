@@ -93,7 +93,6 @@ md_status adj_build(md_adjoint* a, const double4* p) {
     MD_CUDA(g.bucket.reserve(n));
     MD_CUDA(g.order.reserve(n));
     MD_CUDA(g.tiles.reserve(scan_tiles_needed(g.ncells)));
-    MD_CUDA(g.max_occ.reserve(1));
     MD_CUDA(cudaMemsetAsync(g.count.p, 0, sizeof(int) * g.ncells, st));
     MD_CUDA(cudaMemsetAsync(g.cursor.p, 0, sizeof(int) * g.ncells, st));
     k_cell_assign<<<blocks_for(n, kThreads), kThreads, 0, st>>>(p, n, inv_cell, g.ncps, g.cell_of.p, g.count.p);
@@ -103,7 +102,7 @@ md_status adj_build(md_adjoint* a, const double4* p) {
     k_cell_scatter<<<blocks_for(n, kThreads), kThreads, 0, st>>>(g.cell_of.p, n, g.start.p, g.cursor.p, g.bucket.p);
     MD_CHECK_LAUNCH();
     k_cell_rank<<<blocks_for(static_cast<long long>(g.ncells) * 32, kThreads), kThreads, 0, st>>>(
-        g.start.p, g.ncells, g.bucket.p, g.order.p, g.max_occ.p);
+        g.start.p, g.ncells, g.bucket.p, g.order.p);
     MD_CHECK_LAUNCH();
     for (int attempt = 0; attempt < 4; ++attempt) {
         MD_CUDA(a->rows.reserve(row_buffer_entries(n, a->cap)));

@@ -43,15 +43,13 @@ __global__ void k_cell_scatter(const int* __restrict__ cell_of, int n, const int
 // order[] lists every cell's particles in increasing index, as the reference's serial scatter does
 // (src/CellList.cpp:48-51). A cell of up to 32 particles is ranked from registers (one index per lane, compared
 // through shuffles); larger cells compare against the bucket in memory.
-// max_occ receives the largest cell occupancy (it sizes the shared-memory tiles).
 __global__ void k_cell_rank(const int* __restrict__ start, int ncells, const uint32_t* __restrict__ bucket,
-                            uint32_t* __restrict__ order, int* __restrict__ max_occ) {
+                            uint32_t* __restrict__ order) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= ncells) return;
     const int s = start[warp];
     const int m = start[warp + 1] - s;
-    if (lane == 0) atomicMax(max_occ, m);
     if (m <= 32) {
         const uint32_t v = lane < m ? bucket[s + lane] : 0xffffffffu;
         int rank = 0;
