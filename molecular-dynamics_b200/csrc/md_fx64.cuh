@@ -80,8 +80,59 @@ __device__ __forceinline__ void fx64_pair(double dx, double dy, double dz, bool 
     }
 }
 
-// Thread per particle over its row (the layout of k_force_fp32_rows), frames gathered from global memory. Row
-// padding entries carry code 31 and are masked.
+// Sums of one 8-entry group in double
+struct DoubleGroupSums {
+    double x = 0.0, y = 0.0, z = 0.0, e = 0.0, w = 0.0;
+};
+
+// One 8-entry group of a row from fixed-point frames through fx64_pair. Row padding entries carry code 31 and
+// are masked (the sentinel's index is n: particle 0's frame is read instead). With kExact the pairs in the
+// shell around r_c take the reference's exact test; without it the group runs branch-free and reports through
+// *shell whether it holds such a pair, in which case the caller runs it again with kExact (the same sequence
+// with the exact decision, so the same sums as a single exact pass).
+template <bool kEnergy, bool kExact>
+__device__ __forceinline__ DoubleGroupSums fx64_group(const uint4& e0, const uint4& e1, const int4& qi,
+                                                      const int4* __restrict__ frames, const int4* s_off,
+                                                      const double4* __restrict__ pos, int i, const Box& box,
+                                                      const Fx64LJ& lj, unsigned& c, bool* shell) {
+    const uint32_t ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+    DoubleGroupSums g;
+    bool sh = false;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const uint32_t e = ent[u];
+        const uint32_t code = e >> kCodeShift;
+        const bool pad = code == kSentinelCode;
+        const int j = pad ? 0 : static_cast<int>(e & kIndexMask);
+        double dx, dy, dz;
+        const double r2 = fixed_separation(qi, frames[j], s_off[code], dx, dy, dz);
+        bool in = !pad && r2 < lj.lj.rc2;
+        const bool near = !pad && fabs(dsub(r2, lj.lj.rc2)) < lj.band;
+        if (kExact) {
+            if (near) in = exact_inside(pos[i], pos[j], box, lj.lj.rc2);
+        } else {
+            sh |= near;
+        }
+        fx64_pair<kEnergy>(dx, dy, dz, in, pad ? 1.0 : r2, lj, g.x, g.y, g.z, g.e, g.w, c);
+    }
+    if (!kExact) *shell = sh;
+    return g;
+}
+
+template <bool kEnergy>
+__device__ __noinline__ DoubleGroupSums fx64_group_exact(const uint4 e0, const uint4 e1, const int4 qi,
+                                                         const int4* __restrict__ frames, const int4* s_off,
+                                                         const double4* __restrict__ pos, int i, const Box box,
+                                                         const Fx64LJ lj, unsigned* c) {
+    unsigned k = 0;
+    const DoubleGroupSums g = fx64_group<kEnergy, true>(e0, e1, qi, frames, s_off, pos, i, box, lj, k, nullptr);
+    *c = k;
+    return g;
+}
+
+// Thread per particle over its row (the layout of k_force_fp32_rows) with the next group's row quads prefetched
+// (streaming loads), frames gathered from global memory; groups run branch-free, a group with a pair in the
+// cutoff shell runs again out of line with the exact test.
 template <bool kEnergy>
 __global__ void __launch_bounds__(128) k_force_fx64_rows(const int4* __restrict__ frames, const double4* __restrict__ pos,
                                                          int n, Box box, Fx64LJ lj, FixedOffsets offs,
@@ -99,25 +150,25 @@ __global__ void __launch_bounds__(128) k_force_fx64_rows(const int4* __restrict_
         const int2 c = counts[i];
         const int groups = (c.x + c.y + 7) >> 3;
         FloatAcc<true, kEnergy> a;
+        const uint4* rq = reinterpret_cast<const uint4*>(rows) + static_cast<size_t>(i >> 5) * (cap >> 2) * 32 + (i & 31);
+        uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
+        if (groups > 0) {
+            n0 = __ldcs(rq);
+            n1 = __ldcs(rq + 32);
+        }
         for (int g = 0; g < groups; ++g) {
-            const uint4 e0 = row_quad(rows, i, 2 * g, cap);
-            const uint4 e1 = row_quad(rows, i, 2 * g + 1, cap);
-            const uint32_t ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
-            double gx = 0.0, gy = 0.0, gz = 0.0, ge = 0.0, gw = 0.0;
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const uint32_t e = ent[u];
-                const uint32_t code = e >> kCodeShift;
-                // the sentinel's index is n: read particle 0's frame instead (masked below)
-                const int j = code == kSentinelCode ? 0 : static_cast<int>(e & kIndexMask);
-                double dx, dy, dz;
-                const double r2 = fixed_separation(qi, frames[j], s_off[code], dx, dy, dz);
-                bool in = code != kSentinelCode && r2 < lj.lj.rc2;
-                if (code != kSentinelCode && fabs(dsub(r2, lj.lj.rc2)) < lj.band)
-                    in = exact_inside(pos[i], pos[j], box, lj.lj.rc2);
-                fx64_pair<kEnergy>(dx, dy, dz, in, code == kSentinelCode ? 1.0 : r2, lj, gx, gy, gz, ge, gw, ins);
+            const uint4 e0 = n0, e1 = n1;
+            rq += 64;
+            if (g + 1 < groups) {
+                n0 = __ldcs(rq);
+                n1 = __ldcs(rq + 32);
             }
-            a.add_group(gx, gy, gz, ge, gw, e_fx, w_fx);
+            unsigned gin = 0;
+            bool shell = false;
+            DoubleGroupSums gs = fx64_group<kEnergy, false>(e0, e1, qi, frames, s_off, pos, i, box, lj, gin, &shell);
+            if (shell) gs = fx64_group_exact<kEnergy>(e0, e1, qi, frames, s_off, pos, i, box, lj, &gin);
+            ins += gin;
+            a.add_group(gs.x, gs.y, gs.z, gs.e, gs.w, e_fx, w_fx);
         }
         k_fx = a.finish(i, n, force, kick);
     }
