@@ -518,9 +518,19 @@ def run_gpu_arm(a):
         return
     peak, peak_src = measured_peak()
     kernel_s = (force_ms / max(force_n, 1)) / 1e3
-    bytes_per_atom = 16 + 24 + 4 * 2 * pairs / n  # own float4, fixed-point force, full-list int32 indices
+    # DRAM bytes per atom of one force launch: the particle's own coordinates, its force, the full-list int32
+    # indices (neighbour coordinates are gathered through L1/L2 and counted once, in the own term), the fused
+    # closing kick (velocity read and write, mass) and, in the float modes, the fused next kick and drift
+    # (position in and out, reference position, build cell, new float frame); FP64 adds its own-pair (E, W)
+    # records for the ordered energy sums.
+    own = 32 if a.precision == "fp64" else 16
+    bytes_per_atom = own + 24 + 4 * 2 * pairs / n + 56
+    if a.precision in ("fp32fx", "fp32"):
+        bytes_per_atom += 32 + 32 + 4 + 32 + 16
+    if a.precision == "fp64":
+        bytes_per_atom += 16 * pairs / n
     achieved = bytes_per_atom * n / kernel_s / 1e9
-    tpa = ncu_traffic_per_atom()
+    tpa = ncu_traffic_per_atom() if a.precision == "fp32fx" else None
     value = replica_throughput(world, n, a.steps, ms)
     line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",

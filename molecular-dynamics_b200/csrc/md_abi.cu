@@ -168,6 +168,7 @@ struct md_nlist {
     DevBuf<long long> half_off, rev_off, tiles;
     DevBuf<double4> ref_pos;
     DevBuf<float4> frames;  // per-particle float coordinates for the float kernels (n + 1, sentinel last)
+    DevBuf<float4> frames2; // the frames a force kernel with the fused next drift writes (then swapped in)
     DevBuf<int4> iframes;   // fixed-point frames of MD_PREC_FX64 (n)
     bool use_tiles = false; // shared-memory tile kernels (3+ cells per side and tiles that fit)
     TileGeom tiles_geom{};
@@ -446,7 +447,7 @@ bool nlist_current(const md_nlist* nl, const md_system* s) {
 
 // Defined in md_abi_float.inl and below
 md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt,
-                                  bool frames_fresh, bool* fused_ke);
+                                  bool frames_fresh, bool* fused_ke, bool fuse_drift);
 md_status rdf_sample_async(md_rdf* r, md_system* s, md_nlist* nl);
 md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
                     const md_run_options& o, double* pe, double* ke, double* virial);
@@ -532,8 +533,11 @@ md_status choose_variant(md_system* s, md_nlist* nl, int prec, Launch&& launch) 
 // them). Returns through *fused_ke whether the fused kick also left the step's kinetic energy in
 // s->scal[kScalKE] (float tile kernels only; fixed-point, not the reference's summation order).
 md_status kick_async(md_system* s, double dt);
+// With fuse_drift (float modes on a tiled list, with the closing kick) the kernel also performs the next step's
+// opening kick and drift (KickArgs), leaving the new positions and frames in place and the half-skin flag in
+// nl->flags[0].
 md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt = 0.0,
-                            bool frames_fresh = false, bool* fused_ke = nullptr) {
+                            bool frames_fresh = false, bool* fused_ke = nullptr, bool fuse_drift = false) {
     const int n = static_cast<int>(s->n);
     if (fused_ke) *fused_ke = false;
     MD_CUDA(ff->out.reserve(4));
@@ -584,7 +588,7 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
             }
         }
     } else {
-        MD_TRY(forces_list_float_async(ff, s, nl, want_energy, kick_dt, frames_fresh, fused_ke));
+        MD_TRY(forces_list_float_async(ff, s, nl, want_energy, kick_dt, frames_fresh, fused_ke, fuse_drift));
     }
     return MD_OK;
 }

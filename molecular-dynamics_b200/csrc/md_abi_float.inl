@@ -114,7 +114,7 @@ md_status forces_list_fx64_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
 
 // See forces_list_async. Every float kernel fuses the closing kick with a fixed-point kinetic energy.
 md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt,
-                                  bool frames_fresh, bool* fused_ke) {
+                                  bool frames_fresh, bool* fused_ke, bool fuse_drift) {
     if (ff->precision == MD_PREC_FX64) return forces_list_fx64_async(ff, s, nl, want_energy, kick_dt, fused_ke);
     const int n = static_cast<int>(s->n);
     const bool fixed = ff->precision == MD_PREC_FP32FX;
@@ -132,9 +132,12 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
             const TileGeom& tg = nl->tiles_geom;
             const CellOffsets offs = cell_offsets(nl, s);
             const size_t smem = sizeof(float4) * (tg.max_staged + 1);
-            auto launch = [&](int variant, bool with_kick, bool energy, double* tune_vel = nullptr) -> md_status {
-                const KickArgs ka = tune_vel ? KickArgs{tune_vel, s->mass.p, 0.0}
-                                             : KickArgs{with_kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
+            KickArgs drift{nullptr, nullptr, 0.0};
+            auto launch = [&](int variant, bool with_kick, bool energy, double* tune_vel = nullptr,
+                              const KickArgs* fused = nullptr) -> md_status {
+                const KickArgs ka = fused ? *fused
+                                          : tune_vel ? KickArgs{tune_vel, s->mass.p, 0.0}
+                                                     : KickArgs{with_kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
                 auto go = [&](auto rows_kernel, auto tile_kernel, auto prefetch_kernel,
                               auto capped_kernel) -> md_status {
                     if (variant == 1) {
@@ -173,7 +176,30 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
             MD_TRY(choose_variant(s, nl, ff->precision, [&](int v) { return launch(v, true, true, s->vel2.p); }));
             if (want_energy || kick) MD_CUDA(cudaMemsetAsync(ff->fx_acc.p, 0, 4 * sizeof(long long), s->stream));
             MD_TRY(profile_mark(s));
-            MD_TRY(launch(nl->variant[ff->precision], kick, want_energy));
+            if (fuse_drift && kick && nl->use_tiles) {
+                // the next step's kick and drift in the same kernel: new positions and frames go to the spare
+                // buffers (the force loop reads the current ones) and are swapped in after the launch
+                MD_CUDA(s->pos2.reserve(n));
+                MD_CUDA(nl->frames2.reserve(static_cast<size_t>(n) + 1));
+                MD_CUDA(cudaMemsetAsync(nl->flags.p, 0, sizeof(int), s->stream));
+                drift = KickArgs{s->vel.p, s->mass.p, 0.5 * kick_dt};
+                drift.pos_in = s->pos.p;
+                drift.pos_out = s->pos2.p;
+                drift.frames_out = nl->frames2.p;
+                drift.ref_pos = nl->ref_pos.p;
+                drift.max_disp2 = nl->max_disp2;
+                drift.stale = nl->flags.p;
+                drift.cell_sorted = nl->cell_sorted.p;
+                drift.ncps = tg.ncps;
+                drift.cell = tg.cell;
+                drift.dt = kick_dt;
+                drift.box = s->box;
+                MD_TRY(launch(nl->variant[ff->precision], kick, want_energy, nullptr, &drift));
+                swap_buffers(s->pos, s->pos2);
+                swap_buffers(nl->frames, nl->frames2);
+            } else {
+                MD_TRY(launch(nl->variant[ff->precision], kick, want_energy));
+            }
             MD_TRY(profile_mark(s));
         } else {
             const KickArgs ka{kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
@@ -264,11 +290,28 @@ md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, in
     if (n_steps > 0) MD_CUDA(rec.reserve(3 * static_cast<size_t>(n_steps)));
     const bool want_energy = pe || virial;
     const bool exact_ke = ff->precision == MD_PREC_FP64;
+    const bool float_mode = ff->precision == MD_PREC_FP32FX || ff->precision == MD_PREC_FP32;
+    bool drifted = false;  // the previous step's force kernel already made this step's kick and drift
     for (int64_t k = 0; k < n_steps; ++k) {
         const int64_t step = o.first_step + k;
         bool rebuilt = false, fused_ke = false;
-        MD_TRY(drift_and_update(s, ff, nl, dt, &rebuilt));
-        MD_TRY(forces_list_async(ff, s, nl, want_energy, dt, true, &fused_ke));
+        if (drifted) {
+            int flag = 0;
+            MD_CUDA(cudaMemcpyAsync(&flag, nl->flags.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+            MD_TRY(sync(s));
+            if (flag != 0) MD_TRY(nlist_build(nl, s));
+            rebuilt = flag != 0;
+        } else {
+            MD_TRY(drift_and_update(s, ff, nl, dt, &rebuilt));
+        }
+        // fuse the next step's kick and drift unless something touches velocities or positions in between
+        const bool thermostat_now = (o.thermostat == 1 && o.rescale_every > 0 && step % o.rescale_every == 0) ||
+                                    o.thermostat == 2;
+        const bool rdf_now = o.rdf && o.rdf_every > 0 && step % o.rdf_every == 0;
+        const bool fuse = float_mode && k + 1 < n_steps && !thermostat_now && !rdf_now && nl->use_tiles &&
+                          nlist_current(nl, s);
+        MD_TRY(forces_list_async(ff, s, nl, want_energy, dt, true, &fused_ke, fuse));
+        drifted = fuse;
         if (want_energy)
             MD_CUDA(cudaMemcpyAsync(rec.p + 3 * k, ff->out.p, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
         bool ke_current = fused_ke && !exact_ke;  // scal[kScalKE] holds this step's kinetic energy

@@ -41,15 +41,40 @@ struct FloatLJ {
     double rc2d;   // cut_off^2 in double
 };
 
+// The frame of a position: minimum-image (r - centre of cell c), narrowed to float. Every kernel that writes
+// frames calls this, with explicit roundings, so all of them produce the same bits.
+__device__ __forceinline__ float4 frame_of(const double4& p, int c, int ncps, double cell, const Box& box) {
+    const int cx = c / (ncps * ncps), cy = (c / ncps) % ncps, cz = c % ncps;
+    double d[3] = {dsub(p.x, dmul(cx + 0.5, cell)), dsub(p.y, dmul(cy + 0.5, cell)), dsub(p.z, dmul(cz + 0.5, cell))};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d[k] = dsub(d[k], dmul(box.L, rint(dmul(d[k], box.invL))));
+    return make_float4(static_cast<float>(d[0]), static_cast<float>(d[1]), static_cast<float>(d[2]), 0.0f);
+}
+
 struct CellOffsets {
     float4 off[32];  // -d * cell for the 27 codes (d in {-1, 0, 1}^3); zero for the sentinel code
 };
 
-// The closing half kick fused into a force kernel (vel == nullptr: forces only)
+// The closing half kick fused into a force kernel (vel == nullptr: forces only). With pos_out set, the next
+// step's opening kick and drift are fused too (a step whose velocities nothing else touches in between): the
+// kernel writes v + (half_dt F) / m once more, the new positions into pos_out and their float frames into
+// frames_out (the force loop still reads the old ones), and runs the half-skin test against ref_pos into
+// *stale, with k_kick_drift_frames' operation sequence.
 struct KickArgs {
     double* vel;
     const double* mass;
     double half_dt;
+    const double4* pos_in = nullptr;
+    double4* pos_out = nullptr;
+    float4* frames_out = nullptr;
+    const double4* ref_pos = nullptr;
+    double max_disp2 = 0.0;
+    int* stale = nullptr;
+    const int* cell_sorted = nullptr;
+    int ncps = 0;
+    double cell = 0.0;
+    double dt = 0.0;
+    Box box{};
 };
 
 // The truncated potential's force jumps by |F(r_c)| at the cutoff, so a pair whose float r^2 sits within
@@ -192,15 +217,34 @@ struct FloatAcc {
                              kFixed ? static_cast<double>(ay) * kForceUnit : static_cast<double>(fy),
                              kFixed ? static_cast<double>(az) * kForceUnit : static_cast<double>(fz)};
         double ke = 0.0;
+        double vn[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             const size_t o = static_cast<size_t>(k) * n + i;
             force[o] = F[k];
             if (kick.vel) {  // VelocityVerletIntegrator::kick (src/Integrator.cpp:55-71)
                 const double v = dadd(kick.vel[o], ddiv(dmul(kick.half_dt, F[k]), kick.mass[i]));
-                kick.vel[o] = v;
                 ke = dadd(ke, dmul(v, v));
+                if (kick.pos_out) {  // the next step's kickAndDrift (src/Integrator.cpp:32-53)
+                    vn[k] = dadd(v, ddiv(dmul(kick.half_dt, F[k]), kick.mass[i]));
+                    kick.vel[o] = vn[k];
+                } else {
+                    kick.vel[o] = v;
+                }
             }
+        }
+        if (kick.vel && kick.pos_out) {
+            double4 p = kick.pos_in[i];
+            p.x = wrap(dadd(p.x, dmul(kick.dt, vn[0])), kick.box);
+            p.y = wrap(dadd(p.y, dmul(kick.dt, vn[1])), kick.box);
+            p.z = wrap(dadd(p.z, dmul(kick.dt, vn[2])), kick.box);
+            kick.pos_out[i] = p;
+            const double4 r = kick.ref_pos[i];  // NeighbourList::update (src/NeighbourList.cpp:24-30)
+            const double dx = min_image(dsub(p.x, r.x), kick.box);
+            const double dy = min_image(dsub(p.y, r.y), kick.box);
+            const double dz = min_image(dsub(p.z, r.z), kick.box);
+            if (norm2(dx, dy, dz) > kick.max_disp2) *kick.stale = 1;
+            kick.frames_out[i] = frame_of(p, kick.cell_sorted[i], kick.ncps, kick.cell, kick.box);
         }
         return kick.vel ? __double2ll_rn(dmul(dmul(dmul(0.5, kick.mass[i]), ke), kKineticScale)) : 0;
     }
@@ -219,16 +263,6 @@ __device__ __forceinline__ void flush_sums(long long e_fx, long long w_fx, unsig
         if (ins) atomicAdd(&acc[2], ins);
         if (k_fx) atomicAdd(&acc[3], static_cast<unsigned long long>(k_fx));
     }
-}
-
-// The frame of a position: minimum-image (r - centre of cell c), narrowed to float. Every kernel that writes
-// frames calls this, with explicit roundings, so all of them produce the same bits.
-__device__ __forceinline__ float4 frame_of(const double4& p, int c, int ncps, double cell, const Box& box) {
-    const int cx = c / (ncps * ncps), cy = (c / ncps) % ncps, cz = c % ncps;
-    double d[3] = {dsub(p.x, dmul(cx + 0.5, cell)), dsub(p.y, dmul(cy + 0.5, cell)), dsub(p.z, dmul(cz + 0.5, cell))};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) d[k] = dsub(d[k], dmul(box.L, rint(dmul(d[k], box.invL))));
-    return make_float4(static_cast<float>(d[0]), static_cast<float>(d[1]), static_cast<float>(d[2]), 0.0f);
 }
 
 // The image offset -d * cell of a neighbour-cell code (d in {-1, 0, 1}^3), zero for codes above 26: the same
@@ -268,6 +302,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_force_fp32_rows(const float
     if (threadIdx.x < 32) s_off[threadIdx.x] = offs.off[threadIdx.x];
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (kick.frames_out && i == 0) kick.frames_out[n] = make_float4(kSentinelCoord, kSentinelCoord, kSentinelCoord, 0.0f);
     long long e_fx = 0, w_fx = 0, k_fx = 0;
     unsigned ins = 0;
     if (i < n) {

@@ -308,6 +308,8 @@ __global__ void __launch_bounds__(kTileThreads) k_force_fp32_tile(
     extern __shared__ float4 s_q[];
     __shared__ TileTables t;
     __shared__ float4 s_tab[kMaxSegment][32];
+    if (kick.frames_out && blockIdx.x == 0 && threadIdx.x == 0)
+        kick.frames_out[n_atoms] = make_float4(kSentinelCoord, kSentinelCoord, kSentinelCoord, 0.0f);
     tile_tables(g, cell_start, t);
     const int span = t.kk + 2;
     const int sentinel_slot = g.max_staged;

@@ -461,6 +461,55 @@ def test_list_build_variants_agree(md, cells, density, temperature, skin):
             assert np.array_equal(d[k], out[0][3][k]), k
 
 
+@pytest.mark.parametrize("prec", ["PREC_FP32FX", "PREC_FP32"])
+def test_fused_next_drift_matches_separate_steps(md, prec):
+    """md_run fuses each NVE step's closing kick with the next step's opening kick and drift in the float force
+    kernel (new positions and frames into spare buffers, the half-skin test alongside). The trajectory, its
+    energies and its rebuilds equal stepping one md_step_list at a time (separate drift kernel) bit for bit; a
+    rescale step in between breaks the fusion for that step and nothing else changes."""
+    p = getattr(md, prec)
+    base = md.fcc_system(12, 0.8442, 1.3, seed=5)
+    st = base.download()
+    runs = []
+    for fused in (True, False):
+        s = md.System.from_arrays(st["pos"], base.box, vel=st["vel"])
+        nl = md.NeighbourList(2.5, 0.3)
+        ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=p)
+        nl.build(s)
+        ff.compute_forces(s, nl)
+        integ = md.VelocityVerletIntegrator(0.005)
+        if fused:
+            pe, _, _ = integ.run(s, ff, nl, 120)
+            pe = list(pe)
+        else:
+            pe = [integ.step(s, ff, nl) for _ in range(120)]
+        runs.append((np.array(pe), s.download(), nl.rebuild_count, s.state_hash()))
+    (pa, sa, ra, ha), (pb, sb, rb, hb) = runs
+    assert ra == rb and ra > 2
+    assert np.array_equal(pa, pb)
+    for k in ("pos", "vel", "force"):
+        assert np.array_equal(sa[k], sb[k]), k
+    assert ha == hb
+    # with a rescale every 7 steps, one md_run of 49 steps equals 49 one-step runs (nothing to fuse across)
+    out = []
+    for one_step_calls in (False, True):
+        s = md.System.from_arrays(st["pos"], base.box, vel=st["vel"])
+        nl = md.NeighbourList(2.5, 0.3)
+        ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=p)
+        nl.build(s)
+        ff.compute_forces(s, nl)
+        integ = md.VelocityVerletIntegrator(0.005)
+        if one_step_calls:
+            for k in range(1, 50):
+                integ.run(s, ff, nl, 1, thermostat="rescale", rescale_every=7, rescale_temperature=1.0,
+                          first_step=k, record=False)
+        else:
+            integ.run(s, ff, nl, 49, thermostat="rescale", rescale_every=7, rescale_temperature=1.0, record=False)
+        out.append(s.download())
+    for k in ("pos", "vel"):
+        assert np.array_equal(out[0][k], out[1][k]), k
+
+
 def test_frame_by_id_inverts_the_list_permutation(md):
     """md_system_frame_by_id (writeXyzFrame's data, src/Trajectory.cpp:4-25): after rebuilds have reordered
     the particles, the device gather through the ids equals the host-side inverse permutation."""
