@@ -579,7 +579,8 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
             const int nb = static_cast<int>((pairs + kChunk - 1) / kChunk);
             if (nb > 0) {
                 MD_CUDA(ff->eblocks.reserve(nb));
-                k_pair_block_sums<<<blocks_for(nb, 128), 128, 0, s->stream>>>(ff->pair_ew.p, pairs, ff->eblocks.p, nb);
+                k_pair_block_sums<<<blocks_for(nb, 32 * kPairSumWarps), 32 * kPairSumWarps, 0, s->stream>>>(
+                    ff->pair_ew.p, pairs, ff->eblocks.p, nb);
                 MD_CHECK_LAUNCH();
                 k_sum_blocks<<<1, 32, 0, s->stream>>>(ff->eblocks.p, nb, ff->out.p);
                 MD_CHECK_LAUNCH();

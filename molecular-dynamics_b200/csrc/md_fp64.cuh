@@ -79,26 +79,41 @@ constexpr int kEnergyWarps = 4;  // warps per block of the blocked kinetic-energ
 
 // The inner loop of deterministicSum (include/Parallel.hpp:43-46) over the (pairEnergy, pairVirial) array the
 // force kernel stored: block b sums pairs [1024 b, 1024 b + 1024) from 0.0 one after another. One lane per
-// block, so a warp advances 32 blocks' ordered sums together.
-__global__ void k_pair_block_sums(const double2* __restrict__ pair_ew, long long pairs, double2* __restrict__ block_sums,
-                                  int nblocks) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nblocks) return;
+// block, so a warp advances 32 blocks' ordered sums together; the warp stages 32 consecutive records of each of
+// its blocks in shared memory at a time (coalesced 512-byte loads), and each lane then adds its block's 32.
+constexpr int kPairSumWarps = 2;
+__global__ void __launch_bounds__(32 * kPairSumWarps) k_pair_block_sums(const double2* __restrict__ pair_ew,
+                                                                        long long pairs,
+                                                                        double2* __restrict__ block_sums, int nblocks) {
+    __shared__ double2 tile[kPairSumWarps][32][33];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b0 = (blockIdx.x * kPairSumWarps + warp) * 32;  // this warp's first block
+    if (b0 >= nblocks) return;
+    double2(*t)[33] = tile[warp];
+    const int b = b0 + lane;
     const long long k0 = static_cast<long long>(b) * kChunk;
-    const int m = static_cast<int>(pairs - k0 < kChunk ? pairs - k0 : kChunk);
-    const double2* v = pair_ew + k0;
+    const int m = b < nblocks ? static_cast<int>(pairs - k0 < kChunk ? pairs - k0 : kChunk) : 0;
     double se = 0.0, sw = 0.0;
-    for (int t = 0; t < m; ++t) {
-        const double2 x = v[t];
-        se = dadd(se, x.x);
-        sw = dadd(sw, x.y);
+    for (int c = 0; c < kChunk; c += 32) {
+        __syncwarp();
+        for (int r = 0; r < 32; ++r) {  // row r: records [c, c + 32) of block b0 + r, lane = record
+            const long long k = static_cast<long long>(b0 + r) * kChunk + c + lane;
+            t[r][lane] = b0 + r < nblocks && k < pairs ? pair_ew[k] : make_double2(0.0, 0.0);
+        }
+        __syncwarp();
+        const int e = m - c < 32 ? m - c : 32;
+        for (int u = 0; u < e; ++u) {
+            const double2 x = t[lane][u];
+            se = dadd(se, x.x);
+            sw = dadd(sw, x.y);
+        }
     }
-    block_sums[b] = make_double2(se, sw);
+    if (b < nblocks) block_sums[b] = make_double2(se, sw);
 }
 
 // The outer loop of deterministicSum (include/Parallel.hpp:52-56): block sums added in order from 0.0.
 // One warp: the lanes stage 256 values at a time in shared memory (the next chunk's loads in flight while
-// lane 0 adds the current one, one value after another).
+// lane 0 adds the current one, one value after another, reading eight ahead of the adds).
 __global__ void k_sum_blocks(const double2* __restrict__ block_sums, int nblocks, double* __restrict__ out) {
     constexpr int kStage = 256;
     __shared__ double2 stage[kStage];
@@ -122,7 +137,18 @@ __global__ void k_sum_blocks(const double2* __restrict__ block_sums, int nblocks
         if (c + 1 < chunks) fetch(c + 1);
         if (lane == 0) {
             const int m = nblocks - c * kStage < kStage ? nblocks - c * kStage : kStage;
-            for (int t = 0; t < m; ++t) {
+            int t = 0;
+            for (; t + 8 <= m; t += 8) {
+                double2 x[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) x[u] = stage[t + u];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    se = dadd(se, x[u].x);
+                    sw = dadd(sw, x[u].y);
+                }
+            }
+            for (; t < m; ++t) {
                 const double2 x = stage[t];
                 se = dadd(se, x.x);
                 sw = dadd(sw, x.y);
