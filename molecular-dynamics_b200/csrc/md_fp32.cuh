@@ -291,6 +291,50 @@ __global__ void k_frames(const double4* __restrict__ pos, int n, const int* __re
 // group's entries are in flight while the current group's frames are gathered, and the streamed rows do not
 // displace the frames from L1/L2. kMinBlocks > 1 (variant 3) caps the registers so that many blocks stay resident
 // on an SM. Same arithmetic, same bits.
+// The row loop of one particle: adds its energy, virial and inside count to the thread's sums and returns its
+// fixed-point kinetic energy after the fused kick.
+template <bool kFixed, bool kEnergy, bool kPrefetch>
+__device__ __forceinline__ long long fp32_row(int i, const float4* __restrict__ frames, const double4* __restrict__ pos,
+                                              int n, const Box& box, const FloatLJ& lj, const float4* s_off,
+                                              const uint32_t* __restrict__ rows, int cap,
+                                              const int2* __restrict__ counts, double* __restrict__ force,
+                                              const KickArgs& kick, long long& e_fx, long long& w_fx, unsigned& ins) {
+    const float4 qi = frames[i];
+    const int2 c = counts[i];
+    const int groups = (c.x + c.y + 7) >> 3;  // rows are padded with sentinels to a multiple of 8
+    FloatAcc<kFixed, kEnergy> a;
+    // quad q of this particle's interleaved row is rq[32 q]; a group is two quads
+    const uint4* rq = reinterpret_cast<const uint4*>(rows) + static_cast<size_t>(i >> 5) * (cap >> 2) * 32 + (i & 31);
+    uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
+    if (kPrefetch && groups > 0) {
+        n0 = __ldcs(rq);
+        n1 = __ldcs(rq + 32);
+    }
+    for (int g = 0; g < groups; ++g) {
+        uint4 e0, e1;
+        if (kPrefetch) {
+            e0 = n0;
+            e1 = n1;
+            rq += 64;
+            if (g + 1 < groups) {
+                n0 = __ldcs(rq);
+                n1 = __ldcs(rq + 32);
+            }
+        } else {
+            e0 = rq[64 * g];
+            e1 = rq[64 * g + 32];
+        }
+        const GroupSums gs = float_group<kEnergy>(
+            e0, e1, lj,
+            [=](uint32_t e, float& dx, float& dy, float& dz) {
+                return float_separation(qi, frames[e & kIndexMask], s_off[e >> kCodeShift], dx, dy, dz);
+            },
+            [=](uint32_t e) { return exact_inside(pos[i], pos[e & kIndexMask], box, lj.rc2d); }, ins);
+        a.add_group(gs.x, gs.y, gs.z, gs.e, gs.w, e_fx, w_fx);
+    }
+    return a.finish(i, n, force, kick);
+}
+
 template <bool kFixed, bool kEnergy, bool kPrefetch = false, int kMinBlocks = 1>
 __global__ void __launch_bounds__(128, kMinBlocks) k_force_fp32_rows(const float4* __restrict__ frames,
                                                          const double4* __restrict__ pos, int n, Box box,
@@ -305,42 +349,9 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_force_fp32_rows(const float
     if (kick.frames_out && i == 0) kick.frames_out[n] = make_float4(kSentinelCoord, kSentinelCoord, kSentinelCoord, 0.0f);
     long long e_fx = 0, w_fx = 0, k_fx = 0;
     unsigned ins = 0;
-    if (i < n) {
-        const float4 qi = frames[i];
-        const int2 c = counts[i];
-        const int groups = (c.x + c.y + 7) >> 3;  // rows are padded with sentinels to a multiple of 8
-        FloatAcc<kFixed, kEnergy> a;
-        // quad q of this particle's interleaved row is rq[32 q]; a group is two quads
-        const uint4* rq = reinterpret_cast<const uint4*>(rows) + static_cast<size_t>(i >> 5) * (cap >> 2) * 32 + (i & 31);
-        uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
-        if (kPrefetch && groups > 0) {
-            n0 = __ldcs(rq);
-            n1 = __ldcs(rq + 32);
-        }
-        for (int g = 0; g < groups; ++g) {
-            uint4 e0, e1;
-            if (kPrefetch) {
-                e0 = n0;
-                e1 = n1;
-                rq += 64;
-                if (g + 1 < groups) {
-                    n0 = __ldcs(rq);
-                    n1 = __ldcs(rq + 32);
-                }
-            } else {
-                e0 = rq[64 * g];
-                e1 = rq[64 * g + 32];
-            }
-            const GroupSums gs = float_group<kEnergy>(
-                e0, e1, lj,
-                [=](uint32_t e, float& dx, float& dy, float& dz) {
-                    return float_separation(qi, frames[e & kIndexMask], s_off[e >> kCodeShift], dx, dy, dz);
-                },
-                [=](uint32_t e) { return exact_inside(pos[i], pos[e & kIndexMask], box, lj.rc2d); }, ins);
-            a.add_group(gs.x, gs.y, gs.z, gs.e, gs.w, e_fx, w_fx);
-        }
-        k_fx = a.finish(i, n, force, kick);
-    }
+    if (i < n)
+        k_fx = fp32_row<kFixed, kEnergy, kPrefetch>(i, frames, pos, n, box, lj, s_off, rows, cap, counts, force, kick,
+                                                    e_fx, w_fx, ins);
     if (kEnergy || kick.vel) flush_sums(e_fx, w_fx, ins, k_fx, acc);
 }
 
