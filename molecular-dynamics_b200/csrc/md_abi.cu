@@ -189,7 +189,14 @@ struct md_forcefield {
     double virial = 0.0, inside = 0.0;
     int device = -1;
     DevBuf<double2> eblocks;
-    DevBuf<double2> pair_ew;  // FP64 energies: (pairEnergy, pairVirial) of every own pair, in pair order
+    // FP64 energies: (pairEnergy, pairVirial) of every own pair, in pair order, in two buffers used in turn: the
+    // ordered sums of one step run on a second stream (side) while the next step's force kernel fills the other
+    DevBuf<double2> pair_ew[2];
+    int ew_next = 0;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_force = nullptr, ev_done = nullptr, ev_read[2] = {nullptr, nullptr};
+    bool read_pending[2] = {false, false};  // ev_read[b] marks the last sums that read pair_ew[b]
+    bool side_pending = false;              // ev_done marks side-stream sums the system's stream has not joined
     DevBuf<double> out;  // [0] pe, [1] virial, [2] inside
     DevBuf<unsigned long long> inside_count;
     DevBuf<long long> fx_acc;  // fixed-point accumulators of the float kernels: pe, virial
@@ -533,6 +540,21 @@ md_status choose_variant(md_system* s, md_nlist* nl, int prec, Launch&& launch) 
 // them). Returns through *fused_ke whether the fused kick also left the step's kinetic energy in
 // s->scal[kScalKE] (float tile kernels only; fixed-point, not the reference's summation order).
 md_status kick_async(md_system* s, double dt);
+// The system's stream waits for the FP64 energy sums queued on the force field's second stream (every reader or
+// writer of ff->out on the system's stream calls this first)
+md_status join_energy(md_forcefield* ff, md_system* s) {
+    if (ff->side_pending) {
+        MD_CUDA(cudaStreamWaitEvent(s->stream, ff->ev_done, 0));
+        ff->side_pending = false;
+    }
+    return MD_OK;
+}
+
+// The stream on which ff->out is final after the last force call: the second stream while its sums are pending
+cudaStream_t energy_stream(const md_forcefield* ff, const md_system* s) {
+    return ff->side_pending ? ff->side : s->stream;
+}
+
 // With fuse_drift (float modes on a tiled list, with the closing kick) the kernel also performs the next step's
 // opening kick and drift (KickArgs), leaving the new positions and frames in place and the half-skin flag in
 // nl->flags[0].
@@ -540,15 +562,33 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
                             bool frames_fresh = false, bool* fused_ke = nullptr, bool fuse_drift = false) {
     const int n = static_cast<int>(s->n);
     if (fused_ke) *fused_ke = false;
+    if (ff->precision != MD_PREC_FP64) MD_TRY(join_energy(ff, s));
     MD_CUDA(ff->out.reserve(4));
     MD_CUDA(ff->inside_count.reserve(1));
     MD_CUDA(cudaMemsetAsync(ff->inside_count.p, 0, sizeof(unsigned long long), s->stream));
     if (ff->precision == MD_PREC_FP64) {
+        const long long pairs = n > 0 ? static_cast<long long>(nl->pairs) : 0;
+        const int nb = static_cast<int>((pairs + kChunk - 1) / kChunk);
+        // the (E, W) buffer this step fills: free once the sums that last read it are done
+        const int b = ff->ew_next;
+        if (want_energy && nb > 0) {
+            if (!ff->side) {
+                MD_CUDA(cudaStreamCreateWithFlags(&ff->side, cudaStreamNonBlocking));
+                for (cudaEvent_t* e : {&ff->ev_force, &ff->ev_done, &ff->ev_read[0], &ff->ev_read[1]})
+                    MD_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+            }
+            if (ff->pair_ew[b].count < static_cast<size_t>(pairs) || ff->eblocks.count < static_cast<size_t>(nb)) {
+                // a buffer is about to be replaced: no sums may read it; grow with headroom, since the pair count
+                // drifts up and down from one rebuild to the next
+                MD_CUDA(cudaStreamSynchronize(ff->side));
+                MD_CUDA(ff->pair_ew[b].reserve(static_cast<size_t>(pairs + pairs / 8)));
+                MD_CUDA(ff->eblocks.reserve(static_cast<size_t>(nb + nb / 8 + 1)));
+            }
+            if (ff->read_pending[b]) MD_CUDA(cudaStreamWaitEvent(s->stream, ff->ev_read[b], 0));
+        }
         if (n > 0) {
             // variant 0: global gathers; variant 1: shared-memory tile (both bit-identical). With want_energy the
             // kernel also stores every own pair's (E, W) in pair order for the blocked sums below.
-            const long long pairs = static_cast<long long>(nl->pairs);
-            if (want_energy) MD_CUDA(ff->pair_ew.reserve(static_cast<size_t>(pairs)));
             auto launch = [&](int variant, bool kick, double2* ew) -> md_status {
                 if (variant == 1) {
                     const TileGeom& tg = nl->tiles_geom;
@@ -571,20 +611,27 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
             MD_TRY(choose_variant(s, nl, MD_PREC_FP64, [&](int v) { return launch(v, false, nullptr); }));
             MD_CUDA(cudaMemsetAsync(ff->inside_count.p, 0, sizeof(unsigned long long), s->stream));
             MD_TRY(profile_mark(s));
-            MD_TRY(launch(nl->variant[MD_PREC_FP64], kick_dt > 0.0, want_energy ? ff->pair_ew.p : nullptr));
+            MD_TRY(launch(nl->variant[MD_PREC_FP64], kick_dt > 0.0,
+                          want_energy && nb > 0 ? ff->pair_ew[b].p : nullptr));
             MD_TRY(profile_mark(s));
         }
         if (want_energy) {
-            const long long pairs = n > 0 ? static_cast<long long>(nl->pairs) : 0;
-            const int nb = static_cast<int>((pairs + kChunk - 1) / kChunk);
             if (nb > 0) {
-                MD_CUDA(ff->eblocks.reserve(nb));
-                k_pair_block_sums<<<blocks_for(nb, 32 * kPairSumWarps), 32 * kPairSumWarps, 0, s->stream>>>(
-                    ff->pair_ew.p, pairs, ff->eblocks.p, nb);
+                // the ordered sums on the second stream, after this step's force kernel; the next step goes on
+                MD_CUDA(cudaEventRecord(ff->ev_force, s->stream));
+                MD_CUDA(cudaStreamWaitEvent(ff->side, ff->ev_force, 0));
+                k_pair_block_sums<<<blocks_for(nb, 32 * kPairSumWarps), 32 * kPairSumWarps, 0, ff->side>>>(
+                    ff->pair_ew[b].p, pairs, ff->eblocks.p, nb);
                 MD_CHECK_LAUNCH();
-                k_sum_blocks<<<1, 32, 0, s->stream>>>(ff->eblocks.p, nb, ff->out.p);
+                MD_CUDA(cudaEventRecord(ff->ev_read[b], ff->side));
+                ff->read_pending[b] = true;
+                ff->ew_next = b ^ 1;
+                k_sum_blocks<<<1, 32, 0, ff->side>>>(ff->eblocks.p, nb, ff->out.p);
                 MD_CHECK_LAUNCH();
+                MD_CUDA(cudaEventRecord(ff->ev_done, ff->side));
+                ff->side_pending = true;
             } else {
+                MD_TRY(join_energy(ff, s));
                 MD_CUDA(cudaMemsetAsync(ff->out.p, 0, 2 * sizeof(double), s->stream));
             }
         }
@@ -595,6 +642,7 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
 }
 
 md_status read_energy(md_forcefield* ff, md_system* s, double* pe, double* virial, double* inside) {
+    MD_TRY(join_energy(ff, s));
     unsigned long long ins = 0;
     double out[2] = {0, 0};
     MD_CUDA(cudaMemcpyAsync(out, ff->out.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -1209,6 +1257,12 @@ md_status md_forcefield_create(double epsilon, double sigma, double cutoff, md_f
 md_status md_forcefield_destroy(md_forcefield* ff) {
     if (ff && ff->device >= 0) cudaSetDevice(ff->device);
     if (ff && ff->host_out) cudaFreeHost(ff->host_out);
+    if (ff && ff->side) {
+        cudaStreamSynchronize(ff->side);
+        for (cudaEvent_t e : {ff->ev_force, ff->ev_done, ff->ev_read[0], ff->ev_read[1]})
+            if (e) cudaEventDestroy(e);
+        cudaStreamDestroy(ff->side);
+    }
     delete ff;
     return MD_OK;
 }
@@ -1256,6 +1310,7 @@ md_status md_forces_all_pairs(md_forcefield* ff, md_system* s, double* pe, doubl
     MD_TRY(check_cutoff(ff, s));
     ff->device = s->device;
     const int n = static_cast<int>(s->n);
+    MD_TRY(join_energy(ff, s));
     MD_CUDA(ff->out.reserve(4));
     if (n > 0) {
         k_force_all_pairs<<<blocks_for(n, 128), 128, 0, s->stream>>>(s->pos.p, n, s->box, ff->lj, s->force.p);

@@ -312,8 +312,11 @@ md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, in
                           nlist_current(nl, s);
         MD_TRY(forces_list_async(ff, s, nl, want_energy, dt, true, &fused_ke, fuse));
         drifted = fuse;
-        if (want_energy)
-            MD_CUDA(cudaMemcpyAsync(rec.p + 3 * k, ff->out.p, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+        if (want_energy) {  // on the stream where this step's sums end (FP64: the force field's second stream)
+            const cudaStream_t es = energy_stream(ff, s);
+            MD_CUDA(cudaMemcpyAsync(rec.p + 3 * k, ff->out.p, 2 * sizeof(double), cudaMemcpyDeviceToDevice, es));
+            if (es != s->stream) MD_CUDA(cudaEventRecord(ff->ev_done, es));  // the join covers the copy too
+        }
         bool ke_current = fused_ke && !exact_ke;  // scal[kScalKE] holds this step's kinetic energy
         const bool rescale = o.thermostat == 1 && o.rescale_every > 0 && step % o.rescale_every == 0;
         if (rescale || o.thermostat == 2) {
@@ -337,6 +340,7 @@ md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, in
                                     s->stream));
         }
     }
+    MD_TRY(join_energy(ff, s));
     if (n_steps > 0 && (pe || ke || virial)) {
         std::vector<double> h(3 * static_cast<size_t>(n_steps));
         MD_CUDA(cudaMemcpyAsync(h.data(), rec.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s->stream));
