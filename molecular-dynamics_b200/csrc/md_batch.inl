@@ -61,6 +61,9 @@ struct md_batch {
     };
     std::vector<Variant> variants;
     int variant = 0;
+    // tuned on the replicas' starting state (often a lattice); tuned again once after the first chunk of the
+    // first run, on a state the dynamics has reached, unless md_batch_set_force_variant pinned one
+    bool retuned = false;
     uint64_t launches = 0;
     ~md_batch() {
         for (auto& g : graphs) cudaGraphExecDestroy(g.second.first);
@@ -721,6 +724,7 @@ md_status md_batch_set_force_variant(md_batch* b, int variant) {
     } else {
         b->variant = variant;
     }
+    b->retuned = true;
     b_drop_graphs(b);
     return bsync(b);
 }
@@ -785,6 +789,13 @@ md_status md_batch_run(md_batch* b, int64_t n_steps, double* pe, double* virial,
         if (!ok) return fail(MD_ERR_CAPACITY, "neighbour row capacity could not be met");
         done += len;
         cur = 1 - cur;
+        if (!b->retuned) {  // the forces of the current state, recomputed by each variant with the same bits
+            b->retuned = true;
+            const int before = b->variant;
+            MD_TRY(b_autotune(b));
+            MD_TRY(b_clear_acc(b));
+            if (b->variant != before) b_drop_graphs(b);
+        }
     }
     // apply the last step's pending thermostat scales
     k_b_apply_scale<<<b->tiles, kTile, 0, b->stream>>>(b->reps.p, b->tile_rep.p, b->vel.p, b->scale.p);
