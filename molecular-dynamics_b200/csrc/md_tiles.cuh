@@ -172,6 +172,27 @@ __device__ __noinline__ bool exact_within(const double4& pi, const double4& pj, 
     return norm2(ex, ey, ez) < rl2;
 }
 
+// The exact pass of scan_cell: candidates [u0, u1) decided as the float scan does, except those in the thin shell,
+// which the reference's double test decides; appended from the row length cnt on
+__device__ __noinline__ void rescan_cell_exact(const float4* q, int jbase, int u0, int u1, const float4 qo,
+                                               uint32_t code, float lo, float hi, double rl2, int cap,
+                                               const double4 pi, const double4* __restrict__ pos, const Box box,
+                                               uint32_t* row, int& cnt) {
+    for (int u = u0; u < u1; ++u) {
+        const float4 qj = q[u];
+        const float dx = qo.x - qj.x;
+        const float dy = qo.y - qj.y;
+        const float dz = qo.z - qj.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        bool take = r2 < lo;
+        if (!take && r2 <= hi) take = exact_within(pi, pos[jbase + u], box, rl2);
+        if (take) {
+            if (cnt < cap) row[(cnt >> 2) * 128 + (cnt & 3)] = static_cast<uint32_t>(jbase + u) | (code << kCodeShift);
+            ++cnt;
+        }
+    }
+}
+
 // Appends to a row the candidates u in [u0, u1) of one cell that are within r_l of particle i: candidate u has
 // the float frame q[u] and the index jbase + u, qo = q_i + the cell's image offset (the margin covers the
 // rounding of that hoisted sum), row is particle i's interleaved row (entry s at row[(s >> 2) * 128 + (s & 3)])
@@ -215,19 +236,7 @@ __device__ __forceinline__ void scan_cell(const float4* q, int jbase, int u0, in
     }
     if (shell) {
         cnt = cnt0;
-        for (int u = u0; u < u1; ++u) {
-            const float4 qj = q[u];
-            const float dx = qo.x - qj.x;
-            const float dy = qo.y - qj.y;
-            const float dz = qo.z - qj.z;
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            bool take = r2 < lo;
-            if (!take && r2 <= hi) take = exact_within(pi, pos[jbase + u], box, rl2);
-            if (take) {
-                if (cnt < cap) row[(cnt >> 2) * 128 + (cnt & 3)] = static_cast<uint32_t>(jbase + u) | (code << kCodeShift);
-                ++cnt;
-            }
-        }
+        rescan_cell_exact(q, jbase, u0, u1, qo, code, lo, hi, rl2, cap, pi, pos, box, row, cnt);
     }
 }
 
