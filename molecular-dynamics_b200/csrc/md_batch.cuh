@@ -387,7 +387,8 @@ __global__ void __launch_bounds__(kTile)
             // candidates [j0, j1) of one cell (scan_cell: branch-free float screen, exact shell re-scan);
             // qo = q_i + the cell's image offset, computed once per candidate cell
             auto take = [&](int j0, int j1, uint32_t code, const float4& qo) {
-                scan_cell(frames + j0, j0, 0, j1 - j0, qo, code, bp.lo, bp.hi, bp.rl2, bp.cap, pi, pos, d.box, row, cnt);
+                scan_cell<false>(frames + j0, j0, 0, j1 - j0, qo, code, bp.lo, bp.hi, bp.rl2, bp.cap, pi, pos, d.box, row,
+                                 cnt);
             };
             auto shifted = [&](uint32_t code) {
                 const float4 o = code_offset(static_cast<int>(code), cellf);

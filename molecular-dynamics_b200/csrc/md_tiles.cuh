@@ -200,7 +200,9 @@ __device__ __noinline__ void rescan_cell_exact(const float4* q, int jbase, int u
 // appended with a predicated store, one above hi = r_l^2 + margin is dropped. If any candidate of the cell falls
 // in the thin shell between, the cell is scanned again from its first slot with the reference's exact double
 // test (src/NeighbourList.cpp:38-52) deciding the shell, rewriting the same slots. Entries past cap are counted
-// and not written.
+// and not written. kOutOfLine keeps that re-scan in a separate function (fewer registers in the tiled build's
+// loop; the batch build is faster with it inline).
+template <bool kOutOfLine>
 __device__ __forceinline__ void scan_cell(const float4* q, int jbase, int u0, int u1, const float4& qo, uint32_t code,
                                           float lo, float hi, double rl2, int cap, const double4& pi,
                                           const double4* __restrict__ pos, const Box& box, uint32_t* row, int& cnt) {
@@ -236,7 +238,23 @@ __device__ __forceinline__ void scan_cell(const float4* q, int jbase, int u0, in
     }
     if (shell) {
         cnt = cnt0;
-        rescan_cell_exact(q, jbase, u0, u1, qo, code, lo, hi, rl2, cap, pi, pos, box, row, cnt);
+        if (kOutOfLine) {
+            rescan_cell_exact(q, jbase, u0, u1, qo, code, lo, hi, rl2, cap, pi, pos, box, row, cnt);
+        } else {
+            for (int u = u0; u < u1; ++u) {
+                const float4 qj = q[u];
+                const float dx = qo.x - qj.x;
+                const float dy = qo.y - qj.y;
+                const float dz = qo.z - qj.z;
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                bool take = r2 < lo;
+                if (!take && r2 <= hi) take = exact_within(pi, pos[jbase + u], box, rl2);
+                if (take) {
+                    if (cnt < cap) row[(cnt >> 2) * 128 + (cnt & 3)] = static_cast<uint32_t>(jbase + u) | (code << kCodeShift);
+                    ++cnt;
+                }
+            }
+        }
     }
 }
 
@@ -265,7 +283,7 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
         // this particle's interleaved row: entry s at row[(s >> 2) * 128 + (s & 3)]
         uint32_t* row = rows + static_cast<size_t>(i >> 5) * (bp.cap >> 2) * 128 + (i & 31) * 4;
         auto scan = [&](const float4* q, int gs, int u0, int u1, const float4& qo, uint32_t code) {
-            scan_cell(q, gs, u0, u1, qo, code, bp.rl2_lo, bp.rl2_hi, bp.rl2, bp.cap, pi, pos, g.box, row, cnt);
+            scan_cell<true>(q, gs, u0, u1, qo, code, bp.rl2_lo, bp.rl2_hi, bp.rl2, bp.cap, pi, pos, g.box, row, cnt);
         };
         // own pairs: 27 cells in (dx, dy, dz) order, increasing j inside each (src/CellList.cpp:55-83)
         for (uint32_t code = 0; code < 27; ++code) {
