@@ -170,6 +170,7 @@ struct md_nlist {
     DevBuf<float4> frames;  // per-particle float coordinates for the float kernels (n + 1, sentinel last)
     DevBuf<float4> frames2; // the frames a force kernel with the fused next drift writes (then swapped in)
     DevBuf<int4> iframes;   // fixed-point frames of MD_PREC_FX64 (n)
+    DevBuf<int4> iframes2;  // the fixed-point frames a FX64 force kernel with the fused next drift writes
     bool use_tiles = false; // shared-memory tile kernels (3+ cells per side and tiles that fit)
     TileGeom tiles_geom{};
     int build_kernel = -1;  // list build of the last rebuild: 0 thread per particle, 1 tiles
@@ -454,7 +455,7 @@ bool nlist_current(const md_nlist* nl, const md_system* s) {
 
 // Defined in md_abi_float.inl and below
 md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt,
-                                  bool frames_fresh, bool* fused_ke, bool fuse_drift);
+                                  bool frames_fresh, bool* fused_ke, bool fuse_drift, bool fixed_fresh);
 md_status rdf_sample_async(md_rdf* r, md_system* s, md_nlist* nl);
 md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
                     const md_run_options& o, double* pe, double* ke, double* virial);
@@ -559,7 +560,8 @@ cudaStream_t energy_stream(const md_forcefield* ff, const md_system* s) {
 // opening kick and drift (KickArgs), leaving the new positions and frames in place and the half-skin flag in
 // nl->flags[0].
 md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt = 0.0,
-                            bool frames_fresh = false, bool* fused_ke = nullptr, bool fuse_drift = false) {
+                            bool frames_fresh = false, bool* fused_ke = nullptr, bool fuse_drift = false,
+                            bool fixed_fresh = false) {
     const int n = static_cast<int>(s->n);
     if (fused_ke) *fused_ke = false;
     if (ff->precision != MD_PREC_FP64) MD_TRY(join_energy(ff, s));
@@ -636,7 +638,8 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
             }
         }
     } else {
-        MD_TRY(forces_list_float_async(ff, s, nl, want_energy, kick_dt, frames_fresh, fused_ke, fuse_drift));
+        MD_TRY(forces_list_float_async(ff, s, nl, want_energy, kick_dt, frames_fresh, fused_ke, fuse_drift,
+                                       fixed_fresh));
     }
     return MD_OK;
 }

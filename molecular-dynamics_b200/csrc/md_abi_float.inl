@@ -63,8 +63,10 @@ FixedOffsets fixed_offsets(const md_nlist* nl, const md_system* s) {
 
 // MD_PREC_FX64 list forces: fixed-point frames of the current positions, then the global-gather kernel (or the
 // small-box kernel under 3 cells per side); the closing kick and kinetic energy are fused as in the float modes
+// fixed_fresh: the fixed-point frames already match the positions (the previous force kernel drifted them and
+// there was no rebuild since); fuse_drift: as in forces_list_float_async, writing fixed-point frames
 md_status forces_list_fx64_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt,
-                                 bool* fused_ke) {
+                                 bool* fused_ke, bool fixed_fresh, bool fuse_drift) {
     const int n = static_cast<int>(s->n);
     const bool kick = kick_dt > 0.0;
     const Fx64LJ lj = fx64_lj(ff);
@@ -74,13 +76,32 @@ md_status forces_list_fx64_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
     nl->variant[MD_PREC_FX64] = 0;
     if (n > 0) {
         const unsigned g = blocks_for(n, 128);
-        const KickArgs ka{kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
+        KickArgs ka{kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
         if (nl->use_cells) {
             MD_CUDA(nl->iframes.reserve(n));
-            k_frames_fixed<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(s->pos.p, n, nl->cell_sorted.p,
-                                                                               nl->grid.ncps, cell_side(nl, s), s->box,
-                                                                               nl->iframes.p);
-            MD_CHECK_LAUNCH();
+            if (!fixed_fresh) {
+                k_frames_fixed<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(s->pos.p, n, nl->cell_sorted.p,
+                                                                                   nl->grid.ncps, cell_side(nl, s),
+                                                                                   s->box, nl->iframes.p);
+                MD_CHECK_LAUNCH();
+            }
+            const bool fuse = fuse_drift && kick;
+            if (fuse) {  // the next step's kick and drift, new positions and fixed-point frames to spare buffers
+                MD_CUDA(s->pos2.reserve(n));
+                MD_CUDA(nl->iframes2.reserve(n));
+                MD_CUDA(cudaMemsetAsync(nl->flags.p, 0, sizeof(int), s->stream));
+                ka.pos_in = s->pos.p;
+                ka.pos_out = s->pos2.p;
+                ka.iframes_out = nl->iframes2.p;
+                ka.ref_pos = nl->ref_pos.p;
+                ka.max_disp2 = nl->max_disp2;
+                ka.stale = nl->flags.p;
+                ka.cell_sorted = nl->cell_sorted.p;
+                ka.ncps = nl->grid.ncps;
+                ka.cell = cell_side(nl, s);
+                ka.dt = kick_dt;
+                ka.box = s->box;
+            }
             const FixedOffsets offs = fixed_offsets(nl, s);
             MD_TRY(profile_mark(s));
             if (want_energy)
@@ -89,6 +110,11 @@ md_status forces_list_fx64_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
             else
                 k_force_fx64_rows<false><<<g, 128, 0, s->stream>>>(nl->iframes.p, s->pos.p, n, s->box, lj, offs,
                                                                    nl->rows.p, nl->cap, nl->counts.p, s->force.p, acc, ka);
+            if (fuse) {
+                MD_CHECK_LAUNCH();
+                swap_buffers(s->pos, s->pos2);
+                swap_buffers(nl->iframes, nl->iframes2);
+            }
         } else {
             MD_TRY(profile_mark(s));
             if (want_energy)
@@ -114,8 +140,9 @@ md_status forces_list_fx64_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
 
 // See forces_list_async. Every float kernel fuses the closing kick with a fixed-point kinetic energy.
 md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt,
-                                  bool frames_fresh, bool* fused_ke, bool fuse_drift) {
-    if (ff->precision == MD_PREC_FX64) return forces_list_fx64_async(ff, s, nl, want_energy, kick_dt, fused_ke);
+                                  bool frames_fresh, bool* fused_ke, bool fuse_drift, bool fixed_fresh) {
+    if (ff->precision == MD_PREC_FX64)
+        return forces_list_fx64_async(ff, s, nl, want_energy, kick_dt, fused_ke, fixed_fresh, fuse_drift);
     const int n = static_cast<int>(s->n);
     const bool fixed = ff->precision == MD_PREC_FP32FX;
     const bool kick = kick_dt > 0.0;
@@ -290,7 +317,8 @@ md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, in
     if (n_steps > 0) MD_CUDA(rec.reserve(3 * static_cast<size_t>(n_steps)));
     const bool want_energy = pe || virial;
     const bool exact_ke = ff->precision == MD_PREC_FP64;
-    const bool float_mode = ff->precision == MD_PREC_FP32FX || ff->precision == MD_PREC_FP32;
+    const bool float_mode = ff->precision == MD_PREC_FP32FX || ff->precision == MD_PREC_FP32 ||
+                            ff->precision == MD_PREC_FX64;
     bool drifted = false;  // the previous step's force kernel already made this step's kick and drift
     for (int64_t k = 0; k < n_steps; ++k) {
         const int64_t step = o.first_step + k;
@@ -310,7 +338,9 @@ md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, in
         const bool rdf_now = o.rdf && o.rdf_every > 0 && step % o.rdf_every == 0;
         const bool fuse = float_mode && k + 1 < n_steps && !thermostat_now && !rdf_now && nl->use_tiles &&
                           nlist_current(nl, s);
-        MD_TRY(forces_list_async(ff, s, nl, want_energy, dt, true, &fused_ke, fuse));
+        // FX64's fixed-point frames are current when the previous force kernel wrote them and nothing rebuilt
+        const bool fixed_fresh = drifted && !rebuilt;
+        MD_TRY(forces_list_async(ff, s, nl, want_energy, dt, true, &fused_ke, fuse, fixed_fresh));
         drifted = fuse;
         if (want_energy) {  // on the stream where this step's sums end (FP64: the force field's second stream)
             const cudaStream_t es = energy_stream(ff, s);

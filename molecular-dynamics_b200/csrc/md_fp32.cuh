@@ -51,6 +51,20 @@ __device__ __forceinline__ float4 frame_of(const double4& p, int c, int ncps, do
     return make_float4(static_cast<float>(d[0]), static_cast<float>(d[1]), static_cast<float>(d[2]), 0.0f);
 }
 
+constexpr double kFrameScale = 268435456.0;  // 2^28 fixed-point frame units per unit length
+constexpr double kFrameUnit = 1.0 / 268435456.0;
+
+// frame_of in fixed point: round(q * 2^28) per component (|q| stays below a cell plus half the skin, far
+// inside the int32 range)
+__device__ __forceinline__ int4 fixed_frame_of(const double4& p, int c, int ncps, double cell, const Box& box) {
+    const int cx = c / (ncps * ncps), cy = (c / ncps) % ncps, cz = c % ncps;
+    double d[3] = {dsub(p.x, dmul(cx + 0.5, cell)), dsub(p.y, dmul(cy + 0.5, cell)), dsub(p.z, dmul(cz + 0.5, cell))};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d[k] = dsub(d[k], dmul(box.L, rint(dmul(d[k], box.invL))));
+    return make_int4(__double2int_rn(dmul(d[0], kFrameScale)), __double2int_rn(dmul(d[1], kFrameScale)),
+                     __double2int_rn(dmul(d[2], kFrameScale)), 0);
+}
+
 struct CellOffsets {
     float4 off[32];  // -d * cell for the 27 codes (d in {-1, 0, 1}^3); zero for the sentinel code
 };
@@ -66,7 +80,8 @@ struct KickArgs {
     double half_dt;
     const double4* pos_in = nullptr;
     double4* pos_out = nullptr;
-    float4* frames_out = nullptr;
+    float4* frames_out = nullptr;  // float frames of the new positions (float modes)
+    int4* iframes_out = nullptr;   // fixed-point frames of the new positions (MD_PREC_FX64)
     const double4* ref_pos = nullptr;
     double max_disp2 = 0.0;
     int* stale = nullptr;
@@ -244,7 +259,9 @@ struct FloatAcc {
             const double dy = min_image(dsub(p.y, r.y), kick.box);
             const double dz = min_image(dsub(p.z, r.z), kick.box);
             if (norm2(dx, dy, dz) > kick.max_disp2) *kick.stale = 1;
-            kick.frames_out[i] = frame_of(p, kick.cell_sorted[i], kick.ncps, kick.cell, kick.box);
+            if (kick.frames_out) kick.frames_out[i] = frame_of(p, kick.cell_sorted[i], kick.ncps, kick.cell, kick.box);
+            if (kick.iframes_out)
+                kick.iframes_out[i] = fixed_frame_of(p, kick.cell_sorted[i], kick.ncps, kick.cell, kick.box);
         }
         return kick.vel ? __double2ll_rn(dmul(dmul(dmul(0.5, kick.mass[i]), ke), kKineticScale)) : 0;
     }

@@ -11,20 +11,6 @@
 
 namespace md {
 
-constexpr double kFrameScale = 268435456.0;  // 2^28 fixed-point frame units per unit length
-constexpr double kFrameUnit = 1.0 / 268435456.0;
-
-// frame_of in fixed point: round(q * 2^28) per component (|q| stays below a cell plus half the skin, far
-// inside the int32 range)
-__device__ __forceinline__ int4 fixed_frame_of(const double4& p, int c, int ncps, double cell, const Box& box) {
-    const int cx = c / (ncps * ncps), cy = (c / ncps) % ncps, cz = c % ncps;
-    double d[3] = {dsub(p.x, dmul(cx + 0.5, cell)), dsub(p.y, dmul(cy + 0.5, cell)), dsub(p.z, dmul(cz + 0.5, cell))};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) d[k] = dsub(d[k], dmul(box.L, rint(dmul(d[k], box.invL))));
-    return make_int4(__double2int_rn(dmul(d[0], kFrameScale)), __double2int_rn(dmul(d[1], kFrameScale)),
-                     __double2int_rn(dmul(d[2], kFrameScale)), 0);
-}
-
 __global__ void k_frames_fixed(const double4* __restrict__ pos, int n, const int* __restrict__ cell_sorted, int ncps,
                                double cell, Box box, int4* __restrict__ frames) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;

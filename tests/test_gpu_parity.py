@@ -461,10 +461,10 @@ def test_list_build_variants_agree(md, cells, density, temperature, skin):
             assert np.array_equal(d[k], out[0][3][k]), k
 
 
-@pytest.mark.parametrize("prec", ["PREC_FP32FX", "PREC_FP32"])
+@pytest.mark.parametrize("prec", ["PREC_FP32FX", "PREC_FP32", "PREC_FX64"])
 def test_fused_next_drift_matches_separate_steps(md, prec):
-    """md_run fuses each NVE step's closing kick with the next step's opening kick and drift in the float force
-    kernel (new positions and frames into spare buffers, the half-skin test alongside). The trajectory, its
+    """md_run fuses each NVE step's closing kick with the next step's opening kick and drift in the float and FX64
+    force kernels (new positions and frames into spare buffers, the half-skin test alongside). The trajectory, its
     energies and its rebuilds equal stepping one md_step_list at a time (separate drift kernel) bit for bit; a
     rescale step in between breaks the fusion for that step and nothing else changes."""
     p = getattr(md, prec)
