@@ -29,6 +29,14 @@ struct Fx64LJ {
     double band;   // |r^2 - r_c^2| below this: decide inside/outside with the reference's exact test
 };
 
+// s * 2^-28 in double, exactly, without the conversion unit: the double with high word 0x43300000 and low word
+// s ^ 0x80000000 is 2^52 + 2^31 + s, and one FMA scales it by 2^-28 and removes (2^52 + 2^31) 2^-28 = 16777224
+// (every step exact, so the result is the exact value the int-to-double conversion and the scaling give)
+__device__ __forceinline__ double fixed_to_double(int s) {
+    const double m = __hiloint2double(0x43300000, s ^ static_cast<int>(0x80000000u));
+    return __fma_rn(m, kFrameUnit, -16777224.0);
+}
+
 // Separation of a row entry from fixed-point frames: (q_i - q_j) + offset in wrapping 32-bit arithmetic, then
 // exactly scaled to double; returns r^2
 __device__ __forceinline__ double fixed_separation(const int4& qi, const int4& qj, const int4& o, double& dx, double& dy,
@@ -36,19 +44,27 @@ __device__ __forceinline__ double fixed_separation(const int4& qi, const int4& q
     const int sx = static_cast<int>(static_cast<unsigned>(qi.x) - static_cast<unsigned>(qj.x) + static_cast<unsigned>(o.x));
     const int sy = static_cast<int>(static_cast<unsigned>(qi.y) - static_cast<unsigned>(qj.y) + static_cast<unsigned>(o.y));
     const int sz = static_cast<int>(static_cast<unsigned>(qi.z) - static_cast<unsigned>(qj.z) + static_cast<unsigned>(o.z));
-    dx = dmul(__int2double_rn(sx), kFrameUnit);
-    dy = dmul(__int2double_rn(sy), kFrameUnit);
-    dz = dmul(__int2double_rn(sz), kFrameUnit);
+    dx = fixed_to_double(sx);
+    dy = fixed_to_double(sy);
+    dz = fixed_to_double(sz);
     return __fma_rn(dx, dx, __fma_rn(dy, dy, dmul(dz, dz)));
 }
 
-// One pair's terms in double with a pinned operation sequence: 1/r^2 from the approximate float reciprocal
-// refined by two Newton steps (quadratic convergence from ~2^-23 leaves only the double roundings), then F/r = (48 eps sr6 - 24 eps) sr6 / r^2 and E = 4 eps sr6 (sr6 - 1) - shift
+// The hardware's approximate double reciprocal (PTX rcp.approx.ftz.f64), the seed of 1/r^2
+__device__ __forceinline__ double rcp_approx64(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    return y;
+}
+
+// One pair's terms in double with a pinned operation sequence: 1/r^2 from the approximate double reciprocal
+// refined by two Newton steps (quadratic convergence leaves only the double roundings), then F/r = (48 eps sr6 -
+// 24 eps) sr6 / r^2 and E = 4 eps sr6 (sr6 - 1) - shift
 template <bool kEnergy>
 __device__ __forceinline__ void fx64_pair(double dx, double dy, double dz, bool in, double r2, const Fx64LJ& p,
                                           double& gx, double& gy, double& gz, double& ge, double& gw,
                                           unsigned& ins) {
-    double inv = static_cast<double>(rcp_approx(__double2float_rn(r2)));
+    double inv = rcp_approx64(r2);
     inv = __fma_rn(inv, __fma_rn(-r2, inv, 1.0), inv);
     inv = __fma_rn(inv, __fma_rn(-r2, inv, 1.0), inv);
     const double sr2 = dmul(p.lj.sig2, inv);
