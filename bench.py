@@ -531,6 +531,14 @@ def run_gpu_arm(a):
         bytes_per_atom += 16 * pairs / n
     achieved = bytes_per_atom * n / kernel_s / 1e9
     tpa = ncu_traffic_per_atom() if a.precision == "fp32fx" else None
+    # the FP32-pipe side of the roofline (the force kernel sits between the two): 23 flop per ordered pair of
+    # the full list (separation, r^2, reciprocal, F/r, three accumulating FMAs) and 6 per unordered pair for the
+    # energy and virial, against the nominal FP32 peak (SMs x 128 lanes x 2 flop x the max SM clock sampled)
+    clocks = clk.summary()
+    flops_per_atom = 23 * 2 * pairs / n + 6 * pairs / n
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    fp32_peak = sms * 128 * 2 * clocks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12 if clocks.get("sm_max_mhz") else None
+    fp32_achieved = flops_per_atom * n / kernel_s / 1e12
     value = replica_throughput(world, n, a.steps, ms)
     line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -543,8 +551,11 @@ def run_gpu_arm(a):
                                            2: "global gathers, rows prefetched",
                                            3: "global gathers, rows prefetched, registers capped"}.get(variant, str(variant)),
                          "kernel_ms": kernel_s * 1e3,
-                         "algorithmic_bytes_per_atom": bytes_per_atom, "peak_source": peak_src},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+                         "algorithmic_bytes_per_atom": bytes_per_atom, "peak_source": peak_src,
+                         "fp32": {"flops_per_atom": flops_per_atom, "achieved_tflops": fp32_achieved,
+                                  "nominal_peak_tflops": fp32_peak,
+                                  "frac": None if not fp32_peak else fp32_achieved / fp32_peak}},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "rebuilds": rebuilds, "half_list_pairs": pairs, "max_energy_drift": drift,
             "fp64": fp64, "speedup_vs_fp64": None if fp64 is None else value / world / fp64["value"],
             "other_precisions": others,

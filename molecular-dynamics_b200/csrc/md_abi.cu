@@ -179,6 +179,7 @@ struct md_nlist {
     int pinned[4] = {-1, -1, -1, -1};   // set by md_nlist_set_force_variant
     int rebuilds = 0;
     uint64_t pairs = 0;
+    bool pairs_ready = false;  // half_off and pairs match the last build
     bool built = false;
 };
 
@@ -431,6 +432,21 @@ md_status nlist_build(md_nlist* nl, md_system* s) {
         nl->cap = ((maxrow + maxrow / 4 + 16) + 7) & ~7;
         if (attempt == 3) return fail(MD_ERR_CAPACITY, "neighbour row capacity could not be met");
     }
+    nl->pairs_ready = false;  // the half-list offsets and pair count are computed when first needed
+    nl->n = s->n;
+    nl->sys = s;
+    nl->layout = s->layout;
+    nl->built = true;
+    nl->rebuilds++;
+    return MD_OK;
+}
+
+// The half-list offsets (half_off) and the pair count of the last build: an exclusive scan of the own counts,
+// computed on first use after a build (the FP64 energies, the pair count, the download); float runs never need it
+md_status ensure_pairs(md_nlist* nl) {
+    if (nl->pairs_ready || !nl->built) return MD_OK;
+    md_system* s = const_cast<md_system*>(nl->sys);
+    const int n = static_cast<int>(nl->n);
     if (n > 0) {
         k_own_counts<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(nl->counts.p, n, nl->tmp_counts.p);
         MD_CHECK_LAUNCH();
@@ -441,11 +457,7 @@ md_status nlist_build(md_nlist* nl, md_system* s) {
     MD_CUDA(cudaMemcpyAsync(&pairs, nl->half_off.p + n, sizeof(long long), cudaMemcpyDeviceToHost, s->stream));
     MD_TRY(sync(s));
     nl->pairs = static_cast<uint64_t>(pairs);
-    nl->n = s->n;
-    nl->sys = s;
-    nl->layout = s->layout;
-    nl->built = true;
-    nl->rebuilds++;
+    nl->pairs_ready = true;
     return MD_OK;
 }
 
@@ -569,6 +581,7 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
     MD_CUDA(ff->inside_count.reserve(1));
     MD_CUDA(cudaMemsetAsync(ff->inside_count.p, 0, sizeof(unsigned long long), s->stream));
     if (ff->precision == MD_PREC_FP64) {
+        if (n > 0) MD_TRY(ensure_pairs(nl));
         const long long pairs = n > 0 ? static_cast<long long>(nl->pairs) : 0;
         const int nb = static_cast<int>((pairs + kChunk - 1) / kChunk);
         // the (E, W) buffer this step fills: free once the sums that last read it are done
@@ -1150,7 +1163,13 @@ md_status md_nlist_update(md_nlist* nl, md_system* s, int* rebuilt) {
 md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_count, int* cells_per_side,
                         int* reverse_index) {
     if (!nl) return fail(MD_ERR_INVALID, "null list");
-    if (pair_count) *pair_count = nl->pairs;
+    if (pair_count) {
+        if (nl->built) {
+            MD_TRY(use_system(const_cast<md_system*>(nl->sys)));
+            MD_TRY(ensure_pairs(const_cast<md_nlist*>(nl)));
+        }
+        *pair_count = nl->pairs;
+    }
     if (rebuild_count) *rebuild_count = nl->rebuilds;
     if (cells_per_side) *cells_per_side = nl->grid.ncps;
     if (reverse_index) *reverse_index = nl->reverse ? 1 : 0;
@@ -1201,6 +1220,7 @@ md_status md_nlist_download(md_nlist* nl, uint64_t* offsets, uint64_t* neighbour
     if (!nl) return fail(MD_ERR_INVALID, "null list");
     if (!nl->built) return fail(MD_ERR_STATE, "neighbour list not built");
     MD_TRY(use_system(const_cast<md_system*>(nl->sys)));
+    MD_TRY(ensure_pairs(nl));
     const int n = static_cast<int>(nl->n);
     cudaStream_t st = nl->sys->stream;
     const size_t P = nl->pairs;
