@@ -60,7 +60,8 @@ __device__ __forceinline__ double rcp_approx64(double x) {
 // One pair's terms in double with a pinned operation sequence: 1/r^2 from the approximate double reciprocal
 // (relative error below 2^-19.9, measured on B200 over r^2 in [0.5, 8.5]) refined by two Newton steps (quadratic
 // convergence leaves only the double roundings; one step would already be far below what the 2^-28 frames leave
-// in the force, but measured 11 % slower as compiled), then F/r = (48 eps sr6 - 24 eps) sr6 / r^2 and
+// in the force, but measured 11 % slower as compiled, and the cubic form inv (1 + e + e^2) from one residual e,
+// one FMA fewer, 2 % slower), then F/r = (48 eps sr6 - 24 eps) sr6 / r^2 and
 // E = 4 eps sr6 (sr6 - 1) - shift
 template <bool kEnergy>
 __device__ __forceinline__ void fx64_pair(double dx, double dy, double dz, bool in, double r2, const Fx64LJ& p,

@@ -209,13 +209,15 @@ __device__ __forceinline__ void scan_cell(const float4* q, int jbase, int u0, in
     const int cnt0 = cnt;
     bool shell = false;
     const uint32_t vbase = static_cast<uint32_t>(jbase) | (code << kCodeShift);  // entry of candidate u: vbase + u
+    // q_j - qo: the negation of qo - q_j in every bit (round-to-nearest is symmetric), x and y in one packed add
+    const float2 nxy = make_float2(-qo.x, -qo.y);
+    const float nz = -qo.z;
     if (cnt + (u1 - u0) <= cap) {  // every candidate fits: no capacity test per candidate
         for (int u = u0; u < u1; ++u) {
             const float4 qj = q[u];
-            const float dx = qo.x - qj.x;
-            const float dy = qo.y - qj.y;
-            const float dz = qo.z - qj.z;
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float2 d = __fadd2_rn(make_float2(qj.x, qj.y), nxy);
+            const float dz = __fadd_rn(qj.z, nz);
+            const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, dz * dz));
             const bool take = r2 < lo;
             shell |= !take && r2 <= hi;
             uint32_t* p = row + (cnt + 31 * (cnt & ~3));  // (cnt >> 2) * 128 + (cnt & 3)
@@ -226,10 +228,9 @@ __device__ __forceinline__ void scan_cell(const float4* q, int jbase, int u0, in
     } else {
         for (int u = u0; u < u1; ++u) {
             const float4 qj = q[u];
-            const float dx = qo.x - qj.x;
-            const float dy = qo.y - qj.y;
-            const float dz = qo.z - qj.z;
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float2 d = __fadd2_rn(make_float2(qj.x, qj.y), nxy);
+            const float dz = __fadd_rn(qj.z, nz);
+            const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, dz * dz));
             const bool take = r2 < lo;
             shell |= !take && r2 <= hi;
             if (take && cnt < cap) row[(cnt >> 2) * 128 + (cnt & 3)] = vbase + static_cast<uint32_t>(u);
