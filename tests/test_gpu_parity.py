@@ -13,7 +13,7 @@ import math
 import numpy as np
 import pytest
 
-from oracle.oracle import MODE_ALL_PAIRS, MODE_DETERMINISTIC, ONeighbourList, OForceField
+from oracle.oracle import MODE_ALL_PAIRS, MODE_DETERMINISTIC, ONeighbourList, OForceField, fcc_box
 
 pytestmark = pytest.mark.gpu
 
@@ -391,6 +391,93 @@ def test_larger_systems_match_oracle(md, oracle, cells, density):
     for k in range(50):
         assert off.step(o, onl, 0.005, MODE_DETERMINISTIC) == pe[k], k
         assert o.kinetic() == ke[k]
+    assert s.state_hash() == o.hash()
+    assert nl.rebuild_count == onl.rebuilds
+
+
+def ragged_start(oracle, kind):
+    """Non-uniform starts with empty cells and ragged rows (seeded): 'sparse' keeps 5 % of an FCC 12^3 lattice
+    (rows of 0 to about 10 entries, some particles without neighbours); 'blob' is an FCC 8^3 liquid-density
+    block in a 30-sigma box of vacuum (rows far above the capacity estimated from the mean density, so the
+    build regrows them); 'slab' is the bottom third of an FCC 12^3 lattice; 'no_pairs' is 27 particles 4 sigma
+    apart (every row empty, zero pairs)."""
+    rng = np.random.default_rng({"sparse": 1, "blob": 2, "slab": 3, "no_pairs": 4}[kind])
+    if kind == "sparse":
+        a, box = fcc_box(12, 0.8442)
+        pos = oracle.fcc(12, a)
+        pos = pos[rng.random(len(pos)) < 0.05]
+    elif kind == "blob":
+        a, _ = fcc_box(8, 0.8442)
+        pos = oracle.fcc(8, a)
+        pos[:, :3] += 5.0
+        box = 30.0
+    elif kind == "slab":
+        a, box = fcc_box(12, 0.8442)
+        pos = oracle.fcc(12, a)
+        pos = pos[pos[:, 2] < box / 3.0]
+    else:
+        g = np.arange(3) * 4.0 + 1.0
+        pos = np.array([(x, y, z, 0.0) for x in g for y in g for z in g])
+        box = 12.0
+    vel = rng.normal(0.0, 1.0, (3, len(pos)))
+    return np.ascontiguousarray(pos), float(box), vel
+
+
+@pytest.mark.parametrize("kind", ["sparse", "blob", "slab", "no_pairs"])
+def test_ragged_and_empty_rows_match_oracle(md, oracle, kind):
+    """Empty cells, ragged and empty rows, zero pairs and row-capacity regrowth: both list builds write the
+    reference's lists (src/NeighbourList.cpp:55-134), the deterministic forces, energy, virial and inside count
+    and 30 steps equal the oracle's bit for bit, and the float modes stay within their error bounds of them."""
+    pos, box, vel = ragged_start(oracle, kind)
+    o = oracle.system(pos, box, vel=vel)
+    off = OForceField(oracle, 1.0, 1.0, 2.5)
+    onl = ONeighbourList(oracle, 2.5, 0.3, reverse=True)
+    onl.build(o)
+    pe0 = off.forces(o, onl, MODE_DETERMINISTIC)
+    w0, in0 = off.virial, off.inside
+    st = o.state()
+    Lo = onl.get(o.n)
+    if kind == "no_pairs":
+        assert len(Lo["neighbours"]) == 0 and pe0 == 0.0
+    for variant in (0, 1):
+        s = md.System.from_arrays(pos, box, vel=vel)
+        nl = md.NeighbourList(2.5, 0.3, reverse_index=True)
+        nl.set_build_variant(variant)
+        nl.build(s)
+        assert nl.build_variant() == variant or (variant == 1 and not nl.layout()["use_tiles"])
+        L = nl.download()
+        for k in ("offsets", "neighbours", "rev_offsets", "rev_pairs"):
+            assert np.array_equal(L[k], Lo[k]), (variant, k)
+        ff = md.LennardJonesForceField(1.0, 1.0, 2.5)
+        ff.set_deterministic(True)
+        assert ff.compute_forces(s, nl) == pe0
+        assert ff.virial == w0 and ff.inside_pairs == in0
+        assert np.array_equal(s.forces(), st.force), variant
+    # the float modes from the same start (the build gives the same storage order)
+    rms = float(np.sqrt((st.force ** 2).sum(axis=0).mean()))
+    for prec, bound in ((md.PREC_FP32FX, 2e-4), (md.PREC_FP32, 2e-4), (md.PREC_FX64, 2e-6)):
+        s = md.System.from_arrays(pos, box, vel=vel)
+        nl = md.NeighbourList(2.5, 0.3)
+        nl.build(s)
+        ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)
+        pe = ff.compute_forces(s, nl)
+        dF = np.sqrt(((s.forces() - st.force) ** 2).sum(axis=0))
+        if kind == "no_pairs":
+            assert pe == 0.0 and not s.forces().any(), prec
+        else:
+            assert dF.max() <= bound * rms, (prec, dF.max() / rms)
+            assert abs(pe - pe0) <= 1e-5 * abs(pe0), prec
+    # 30 deterministic steps (rebuilds included) against the oracle's
+    s = md.System.from_arrays(pos, box, vel=vel)
+    nl = md.NeighbourList(2.5, 0.3, reverse_index=True)
+    nl.build(s)
+    ff = md.LennardJonesForceField(1.0, 1.0, 2.5)
+    ff.set_deterministic(True)
+    ff.compute_forces(s, nl)
+    pe, ke, _ = md.VelocityVerletIntegrator(0.005).run(s, ff, nl, 30)
+    for k in range(30):
+        assert off.step(o, onl, 0.005, MODE_DETERMINISTIC) == pe[k], k
+        assert o.kinetic() == ke[k], k
     assert s.state_hash() == o.hash()
     assert nl.rebuild_count == onl.rebuilds
 
