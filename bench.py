@@ -67,7 +67,7 @@ def args_parse():
     p.add_argument("--adjoint-steps", type=int, default=200,
                    help="trajectory length of the differentiation workload (N = 32,000; 0: skip)")
     p.add_argument("--force-variant", type=int, default=-1,
-                   help="list force kernel of the headline run: -1 autotunes, 0-3 pin one (md_nlist_set_force_variant)")
+                   help="list force kernel of the headline run: -1 autotunes, 0-4 pin one (md_nlist_set_force_variant)")
     p.add_argument("--profile-region", action="store_true",
                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return p.parse_args()
@@ -549,7 +549,8 @@ def run_gpu_arm(a):
                          "kernel": {"fp64": "k_force_fp64", "fx64": "k_force_fx64_rows"}.get(a.precision, "k_force_fp32"),
                          "force_variant": {0: "global gathers", 1: "shared-memory tiles",
                                            2: "global gathers, rows prefetched",
-                                           3: "global gathers, rows prefetched, registers capped"}.get(variant, str(variant)),
+                                           3: "global gathers, rows prefetched, registers capped",
+                                           4: "global gathers, rows prefetched, resident grid"}.get(variant, str(variant)),
                          "kernel_ms": kernel_s * 1e3,
                          "algorithmic_bytes_per_atom": bytes_per_atom, "peak_source": peak_src,
                          "fp32": {"flops_per_atom": flops_per_atom, "achieved_tflops": fp32_achieved,

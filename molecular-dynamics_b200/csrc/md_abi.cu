@@ -126,6 +126,8 @@ struct md_system {
     DevBuf<double> frame;
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t frame_ready = nullptr;
+    // resident grid of k_force_fp32_resident<fixed, energy> (blocks that fit on the SMs at once), 0 until known
+    unsigned fp32_resident[2][2] = {{0, 0}, {0, 0}};
 };
 
 // After k_permute: the permuted arrays become the system's, the old ones its reorder buffers. No device
@@ -507,9 +509,9 @@ md_status profile_collect(md_system* s) {
 // choice never changes a result. md_nlist_set_force_variant pins a variant instead.
 template <typename Launch>
 md_status choose_variant(md_system* s, md_nlist* nl, int prec, Launch&& launch) {
-    // variants available: 0 always, 1 with tiles, 2 and 3 (prefetching global gathers, the second with capped
-    // registers) for the float modes
-    unsigned mask = 1u | (nl->use_tiles ? 2u : 0u) | (prec == MD_PREC_FP32FX || prec == MD_PREC_FP32 ? 12u : 0u);
+    // variants available: 0 always, 1 with tiles, 2, 3 and 4 (prefetching global gathers; the second with
+    // capped registers, the third on a resident grid) for the float modes
+    unsigned mask = 1u | (nl->use_tiles ? 2u : 0u) | (prec == MD_PREC_FP32FX || prec == MD_PREC_FP32 ? 28u : 0u);
     if (nl->variant[prec] >= 0 && ((mask >> nl->variant[prec]) & 1u)) return MD_OK;
     if (mask == 1u) {
         nl->variant[prec] = 0;
@@ -524,7 +526,7 @@ md_status choose_variant(md_system* s, md_nlist* nl, int prec, Launch&& launch) 
     MD_CUDA(cudaEventCreate(&e1));
     float best = 0.f;
     int pick = -1;
-    for (int v = 0; v < 4; ++v) {
+    for (int v = 0; v < 5; ++v) {
         if (!((mask >> v) & 1u)) continue;
         MD_TRY(launch(v));
         MD_CUDA(cudaEventRecord(e0, s->stream));
@@ -1177,7 +1179,7 @@ md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_c
 }
 
 md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant) {
-    if (!nl || precision < MD_PREC_FP64 || precision > MD_PREC_FX64 || variant < -1 || variant > 3 ||
+    if (!nl || precision < MD_PREC_FP64 || precision > MD_PREC_FX64 || variant < -1 || variant > 4 ||
         (precision == MD_PREC_FX64 && variant >= 1) || (precision == MD_PREC_FP64 && variant >= 2))
         return fail(MD_ERR_INVALID, "md_nlist_set_force_variant: bad arguments");
     nl->pinned[precision] = variant;

@@ -154,7 +154,8 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
         const unsigned g = blocks_for(n, 128);
         if (nl->use_cells) {
             // variant 0: global gathers (k_force_fp32_rows); 1: shared-memory tile; 2: global gathers with the rows
-            // prefetched a group ahead; 3: as 2 with capped registers (all the same bits)
+            // prefetched a group ahead; 3: as 2 with capped registers; 4: as 2 on a resident grid with split offset
+            // tables (all the same bits)
             if (!frames_fresh) MD_TRY(frames_async(s, nl));
             const TileGeom& tg = nl->tiles_geom;
             const CellOffsets offs = cell_offsets(nl, s);
@@ -165,9 +166,20 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
                 const KickArgs ka = fused ? *fused
                                           : tune_vel ? KickArgs{tune_vel, s->mass.p, 0.0}
                                                      : KickArgs{with_kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
-                auto go = [&](auto rows_kernel, auto tile_kernel, auto prefetch_kernel,
-                              auto capped_kernel) -> md_status {
-                    if (variant == 1) {
+                auto go = [&](auto rows_kernel, auto tile_kernel, auto prefetch_kernel, auto capped_kernel,
+                              auto resident_kernel) -> md_status {
+                    if (variant == 4) {
+                        unsigned& grid = s->fp32_resident[fixed ? 1 : 0][energy ? 1 : 0];
+                        if (grid == 0) {
+                            int sms = 0, per_sm = 0;
+                            MD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+                            MD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, resident_kernel, 128, 0));
+                            grid = static_cast<unsigned>(std::max(1, sms * per_sm));
+                        }
+                        resident_kernel<<<std::min(g, grid), 128, 0, s->stream>>>(
+                            nl->frames.p, s->pos.p, n, s->box, lj, offs, nl->rows.p, nl->cap, nl->counts.p, s->force.p,
+                            acc, ka);
+                    } else if (variant == 1) {
                         if (smem > kSmemNoOptIn)
                             MD_CUDA(cudaFuncSetAttribute(tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                          static_cast<int>(smem)));
@@ -189,13 +201,17 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
                 };
                 if (fixed)
                     return energy ? go(k_force_fp32_rows<true, true>, k_force_fp32_tile<true, true>,
-                                       k_force_fp32_rows<true, true, true>, k_force_fp32_rows<true, true, true, 7>)
+                                       k_force_fp32_rows<true, true, true>, k_force_fp32_rows<true, true, true, 7>,
+                                       k_force_fp32_resident<true, true>)
                                   : go(k_force_fp32_rows<true, false>, k_force_fp32_tile<true, false>,
-                                       k_force_fp32_rows<true, false, true>, k_force_fp32_rows<true, false, true, 7>);
+                                       k_force_fp32_rows<true, false, true>, k_force_fp32_rows<true, false, true, 7>,
+                                       k_force_fp32_resident<true, false>);
                 return energy ? go(k_force_fp32_rows<false, true>, k_force_fp32_tile<false, true>,
-                                   k_force_fp32_rows<false, true, true>, k_force_fp32_rows<false, true, true, 7>)
+                                   k_force_fp32_rows<false, true, true>, k_force_fp32_rows<false, true, true, 7>,
+                                   k_force_fp32_resident<false, true>)
                               : go(k_force_fp32_rows<false, false>, k_force_fp32_tile<false, false>,
-                                   k_force_fp32_rows<false, false, true>, k_force_fp32_rows<false, false, true, 7>);
+                                   k_force_fp32_rows<false, false, true>, k_force_fp32_rows<false, false, true, 7>,
+                                   k_force_fp32_resident<false, false>);
             };
             // tune on the kernel the steps run (energy and the fused kick), the kick writing into the reorder
             // buffer (3n doubles, idle between rebuilds) so the state is untouched

@@ -304,7 +304,7 @@ __global__ void k_frames(const double4* __restrict__ pos, int n, const int* __re
 
 // Thread per particle over its row with neighbour frames gathered from global memory (L1/L2); rows are read
 // as interleaved uint4, coalesced across the warp.
-// kPrefetch (variants 2 and 3): row quads are loaded one group ahead with the streaming cache hint, so the next
+// kPrefetch (variants 2, 3 and 4): row quads are loaded one group ahead with the streaming cache hint, so the next
 // group's entries are in flight while the current group's frames are gathered, and the streamed rows do not
 // displace the frames from L1/L2. kMinBlocks > 1 (variant 3) caps the registers so that many blocks stay resident
 // on an SM. Same arithmetic, same bits.
@@ -350,6 +350,74 @@ __device__ __forceinline__ long long fp32_row(int i, const float4* __restrict__ 
         a.add_group(gs.x, gs.y, gs.z, gs.e, gs.w, e_fx, w_fx);
     }
     return a.finish(i, n, force, kick);
+}
+
+// The row loop of fp32_row with the prefetch, the image offsets read from a table of (x, y) pairs and a table of
+// z (an 8- and a 4-byte shared load per entry instead of one of 16 bytes: fewer shared-memory wavefronts in the
+// L1 data pipe, which the gathers keep busy). Same operations, same bits.
+template <bool kFixed, bool kEnergy>
+__device__ __forceinline__ long long fp32_row_split(int i, const float4* __restrict__ frames,
+                                                    const double4* __restrict__ pos, int n, const Box& box,
+                                                    const FloatLJ& lj, const float2* s_xy, const float* s_z,
+                                                    const uint32_t* __restrict__ rows, int cap,
+                                                    const int2* __restrict__ counts, double* __restrict__ force,
+                                                    const KickArgs& kick, long long& e_fx, long long& w_fx,
+                                                    unsigned& ins) {
+    const float4 qi = frames[i];
+    const int2 c = counts[i];
+    const int groups = (c.x + c.y + 7) >> 3;
+    FloatAcc<kFixed, kEnergy> a;
+    const uint4* rq = reinterpret_cast<const uint4*>(rows) + static_cast<size_t>(i >> 5) * (cap >> 2) * 32 + (i & 31);
+    uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
+    if (groups > 0) {
+        n0 = __ldcs(rq);
+        n1 = __ldcs(rq + 32);
+    }
+    for (int g = 0; g < groups; ++g) {
+        const uint4 e0 = n0, e1 = n1;
+        rq += 64;
+        if (g + 1 < groups) {
+            n0 = __ldcs(rq);
+            n1 = __ldcs(rq + 32);
+        }
+        const GroupSums gs = float_group<kEnergy>(
+            e0, e1, lj,
+            [=](uint32_t e, float& dx, float& dy, float& dz) {
+                const uint32_t k = e >> kCodeShift;
+                const float2 oxy = s_xy[k];
+                return float_separation(qi, frames[e & kIndexMask], make_float4(oxy.x, oxy.y, s_z[k], 0.0f), dx,
+                                        dy, dz);
+            },
+            [=](uint32_t e) { return exact_inside(pos[i], pos[e & kIndexMask], box, lj.rc2d); }, ins);
+        a.add_group(gs.x, gs.y, gs.z, gs.e, gs.w, e_fx, w_fx);
+    }
+    return a.finish(i, n, force, kick);
+}
+
+// Variant 4: fp32_row_split on a resident grid (as many blocks as fit on the SMs at once, each thread taking
+// particles i, i + grid, ...: no block turnover, no partial last wave, one flush of the sums per thread).
+template <bool kFixed, bool kEnergy>
+__global__ void __launch_bounds__(128) k_force_fp32_resident(const float4* __restrict__ frames,
+                                                             const double4* __restrict__ pos, int n, Box box,
+                                                             FloatLJ lj, CellOffsets offs,
+                                                             const uint32_t* __restrict__ rows, int cap,
+                                                             const int2* __restrict__ counts, double* __restrict__ force,
+                                                             unsigned long long* __restrict__ acc, KickArgs kick) {
+    __shared__ __align__(16) float s_o[4][32];  // s_o[0..1]: the 32 (x, y) pairs; s_o[2]: z
+    if (threadIdx.x < 32) {
+        const float4 o = offs.off[threadIdx.x];
+        reinterpret_cast<float2*>(s_o[0])[threadIdx.x] = make_float2(o.x, o.y);
+        s_o[2][threadIdx.x] = o.z;
+    }
+    __syncthreads();
+    if (kick.frames_out && blockIdx.x == 0 && threadIdx.x == 0)
+        kick.frames_out[n] = make_float4(kSentinelCoord, kSentinelCoord, kSentinelCoord, 0.0f);
+    long long e_fx = 0, w_fx = 0, k_fx = 0;
+    unsigned ins = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        k_fx += fp32_row_split<kFixed, kEnergy>(i, frames, pos, n, box, lj, reinterpret_cast<const float2*>(s_o[0]),
+                                                s_o[2], rows, cap, counts, force, kick, e_fx, w_fx, ins);
+    if (kEnergy || kick.vel) flush_sums(e_fx, w_fx, ins, k_fx, acc);
 }
 
 template <bool kFixed, bool kEnergy, bool kPrefetch = false, int kMinBlocks = 1>

@@ -484,7 +484,7 @@ def test_ragged_and_empty_rows_match_oracle(md, oracle, kind):
 
 @pytest.mark.parametrize("cells,density", [(8, 0.8442), (40, 0.8442), (40, 1.0)])
 def test_force_kernel_variants_agree_bit_for_bit(md, cells, density):
-    """The autotuner may pick the global-gather, the shared-memory tile or the prefetching global-gather force
+    """The autotuner may pick the global-gather, the shared-memory tile or a prefetching global-gather force
     kernel; all (and the fused kick) give the same bits in every precision, so the choice never changes a
     trajectory."""
     import numpy as np
@@ -496,7 +496,7 @@ def test_force_kernel_variants_agree_bit_for_bit(md, cells, density):
     st = base.download()
     for prec in (md.PREC_FP64, md.PREC_FP32FX, md.PREC_FP32):
         results = []
-        for variant in ((0, 1) if prec == md.PREC_FP64 else (0, 1, 2, 3)):
+        for variant in ((0, 1) if prec == md.PREC_FP64 else (0, 1, 2, 3, 4)):
             s = md.System.from_arrays(st["pos"], base.box, vel=st["vel"], force=st["force"])
             nl = md.NeighbourList(2.5, 0.3)
             nl.set_force_variant(prec, variant)
