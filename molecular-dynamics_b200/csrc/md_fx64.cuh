@@ -90,14 +90,15 @@ struct DoubleGroupSums {
     double x = 0.0, y = 0.0, z = 0.0, e = 0.0, w = 0.0;
 };
 
-// One 8-entry group of a row from fixed-point frames through fx64_pair. Row padding entries carry code 31 and
+// One 8-entry group of a row from fixed-point frames through fx64_pair (the image offset of code c is
+// (s_xy[c], s_z[c])). Row padding entries carry code 31 and
 // are masked (the sentinel's index is n: particle 0's frame is read instead). With kExact the pairs in the
 // shell around r_c take the reference's exact test; without it the group runs branch-free and reports through
 // *shell whether it holds such a pair, in which case the caller runs it again with kExact (the same sequence
 // with the exact decision, so the same sums as a single exact pass).
 template <bool kEnergy, bool kExact>
 __device__ __forceinline__ DoubleGroupSums fx64_group(const uint4& e0, const uint4& e1, const int4& qi,
-                                                      const int4* __restrict__ frames, const int4* s_off,
+                                                      const int4* __restrict__ frames, const int2* s_xy, const int* s_z,
                                                       const double4* __restrict__ pos, int i, const Box& box,
                                                       const Fx64LJ& lj, unsigned& c, bool* shell) {
     const uint32_t ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
@@ -110,7 +111,8 @@ __device__ __forceinline__ DoubleGroupSums fx64_group(const uint4& e0, const uin
         const bool pad = code == kSentinelCode;
         const int j = pad ? 0 : static_cast<int>(e & kIndexMask);
         double dx, dy, dz;
-        const double r2 = fixed_separation(qi, frames[j], s_off[code], dx, dy, dz);
+        const int2 oxy = s_xy[code];
+        const double r2 = fixed_separation(qi, frames[j], make_int4(oxy.x, oxy.y, s_z[code], 0), dx, dy, dz);
         bool in = !pad && r2 < lj.lj.rc2;
         const bool near = !pad && fabs(dsub(r2, lj.lj.rc2)) < lj.band;
         if (kExact) {
@@ -126,11 +128,11 @@ __device__ __forceinline__ DoubleGroupSums fx64_group(const uint4& e0, const uin
 
 template <bool kEnergy>
 __device__ __noinline__ DoubleGroupSums fx64_group_exact(const uint4 e0, const uint4 e1, const int4 qi,
-                                                         const int4* __restrict__ frames, const int4* s_off,
+                                                         const int4* __restrict__ frames, const int2* s_xy, const int* s_z,
                                                          const double4* __restrict__ pos, int i, const Box box,
                                                          const Fx64LJ lj, unsigned* c) {
     unsigned k = 0;
-    const DoubleGroupSums g = fx64_group<kEnergy, true>(e0, e1, qi, frames, s_off, pos, i, box, lj, k, nullptr);
+    const DoubleGroupSums g = fx64_group<kEnergy, true>(e0, e1, qi, frames, s_xy, s_z, pos, i, box, lj, k, nullptr);
     *c = k;
     return g;
 }
@@ -144,9 +146,18 @@ __global__ void __launch_bounds__(128) k_force_fx64_rows(const int4* __restrict_
                                                          const uint32_t* __restrict__ rows, int cap,
                                                          const int2* __restrict__ counts, double* __restrict__ force,
                                                          unsigned long long* __restrict__ acc, KickArgs kick) {
-    __shared__ int4 s_off[32];
-    if (threadIdx.x < 32) s_off[threadIdx.x] = offs.off[threadIdx.x];
+    // the 32 codes' fixed-point image offsets as a table of (x, y) pairs (s_o[0..1]) and one of z (s_o[2]): an
+    // 8- and a 4-byte shared load per entry instead of one of 16 (fewer shared-memory wavefronts in the L1 data
+    // pipe, which the gathers keep busy)
+    __shared__ __align__(16) int s_o[4][32];
+    if (threadIdx.x < 32) {
+        const int4 o = offs.off[threadIdx.x];
+        reinterpret_cast<int2*>(s_o[0])[threadIdx.x] = make_int2(o.x, o.y);
+        s_o[2][threadIdx.x] = o.z;
+    }
     __syncthreads();
+    const int2* s_xy = reinterpret_cast<const int2*>(s_o[0]);
+    const int* s_z = s_o[2];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     long long e_fx = 0, w_fx = 0, k_fx = 0;
     unsigned ins = 0;
@@ -170,8 +181,8 @@ __global__ void __launch_bounds__(128) k_force_fx64_rows(const int4* __restrict_
             }
             unsigned gin = 0;
             bool shell = false;
-            DoubleGroupSums gs = fx64_group<kEnergy, false>(e0, e1, qi, frames, s_off, pos, i, box, lj, gin, &shell);
-            if (shell) gs = fx64_group_exact<kEnergy>(e0, e1, qi, frames, s_off, pos, i, box, lj, &gin);
+            DoubleGroupSums gs = fx64_group<kEnergy, false>(e0, e1, qi, frames, s_xy, s_z, pos, i, box, lj, gin, &shell);
+            if (shell) gs = fx64_group_exact<kEnergy>(e0, e1, qi, frames, s_xy, s_z, pos, i, box, lj, &gin);
             ins += gin;
             a.add_group(gs.x, gs.y, gs.z, gs.e, gs.w, e_fx, w_fx);
         }
