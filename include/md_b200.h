@@ -149,9 +149,9 @@ md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_c
                         int* reverse_index);
 /* Force kernel choice for one precision: -1 autotunes (the first force call of the list times every
  * available variant and keeps the fastest), 0 pins global gathers, 1 pins the shared-memory tile kernel (used
- * only while the list has tiles; FP64 and the float modes), 2 pins global gathers with the rows prefetched a
- * group ahead, 3 the same with registers capped for occupancy and 4 the same on a resident grid (float modes).
- * Every variant gives the same bits. md_nlist_force_variant reports the variant in use (-1 until the first force call). */
+ * only while the list has tiles; FP64 and the float modes), 2 pins global gathers with the rows prefetched
+ * (FP64: a quad of entries at a time, branch-free; float modes: a group of 8 ahead), 3 the float modes' variant 2
+ * with registers capped for occupancy and 4 the same on a resident grid. Every variant gives the same bits. md_nlist_force_variant reports the variant in use (-1 until the first force call). */
 md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant);
 md_status md_nlist_force_variant(const md_nlist* nl, int precision, int* variant);
 /* List build kernel: -1 uses the shared-memory tile build wherever the list has tiles, 0 pins one thread per

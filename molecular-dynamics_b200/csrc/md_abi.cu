@@ -509,9 +509,10 @@ md_status profile_collect(md_system* s) {
 // choice never changes a result. md_nlist_set_force_variant pins a variant instead.
 template <typename Launch>
 md_status choose_variant(md_system* s, md_nlist* nl, int prec, Launch&& launch) {
-    // variants available: 0 always, 1 with tiles, 2, 3 and 4 (prefetching global gathers; the second with
-    // capped registers, the third on a resident grid) for the float modes
-    unsigned mask = 1u | (nl->use_tiles ? 2u : 0u) | (prec == MD_PREC_FP32FX || prec == MD_PREC_FP32 ? 28u : 0u);
+    // variants available: 0 always, 1 with tiles; for FP64 2 (branch-free quads); for the float modes 2, 3
+    // and 4 (prefetching global gathers; the second with capped registers, the third on a resident grid)
+    unsigned mask = 1u | (nl->use_tiles ? 2u : 0u) | (prec == MD_PREC_FP32FX || prec == MD_PREC_FP32 ? 28u : 0u) |
+                    (prec == MD_PREC_FP64 ? 4u : 0u);
     if (nl->variant[prec] >= 0 && ((mask >> nl->variant[prec]) & 1u)) return MD_OK;
     if (mask == 1u) {
         nl->variant[prec] = 0;
@@ -604,8 +605,9 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
             if (ff->read_pending[b]) MD_CUDA(cudaStreamWaitEvent(s->stream, ff->ev_read[b], 0));
         }
         if (n > 0) {
-            // variant 0: global gathers; variant 1: shared-memory tile (both bit-identical). With want_energy the
-            // kernel also stores every own pair's (E, W) in pair order for the blocked sums below.
+            // variant 0: global gathers; 1: shared-memory tile; 2: global gathers a quad of entries at a time,
+            // branch-free (all bit-identical). With want_energy the kernel also stores every own pair's (E, W) in
+            // pair order for the blocked sums below.
             auto launch = [&](int variant, bool kick, double2* ew) -> md_status {
                 if (variant == 1) {
                     const TileGeom& tg = nl->tiles_geom;
@@ -617,6 +619,10 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
                     k_force_fp64_tile<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
                         s->pos.p, n, nl->grid.start.p, nl->cell_sorted.p, tg, ff->lj, nl->rows.p, nl->cap,
                         nl->counts.p, s->force.p, ff->inside_count.p, ka, nl->half_off.p, ew);
+                } else if (variant == 2) {
+                    k_force_fp64_quads<<<blocks_for(n, 128), 128, 0, s->stream>>>(
+                        s->pos.p, n, s->box, ff->lj, nl->rows.p, nl->cap, nl->counts.p, s->force.p, ff->inside_count.p,
+                        kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt, nl->half_off.p, ew);
                 } else {
                     k_force_fp64<<<blocks_for(n, 128), 128, 0, s->stream>>>(
                         s->pos.p, n, s->box, ff->lj, nl->rows.p, nl->cap, nl->counts.p, s->force.p, ff->inside_count.p,
@@ -1180,7 +1186,7 @@ md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_c
 
 md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant) {
     if (!nl || precision < MD_PREC_FP64 || precision > MD_PREC_FX64 || variant < -1 || variant > 4 ||
-        (precision == MD_PREC_FX64 && variant >= 1) || (precision == MD_PREC_FP64 && variant >= 2))
+        (precision == MD_PREC_FX64 && variant >= 1) || (precision == MD_PREC_FP64 && variant >= 3))
         return fail(MD_ERR_INVALID, "md_nlist_set_force_variant: bad arguments");
     nl->pinned[precision] = variant;
     nl->variant[precision] = -1;

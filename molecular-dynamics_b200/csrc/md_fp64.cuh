@@ -75,6 +75,70 @@ __global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ
     if ((threadIdx.x & 31) == 0 && ins) atomicAdd(inside, ins);
 }
 
+// Variant 2 of k_force_fp64, the same sums without a branch per entry: the row is read a quad (4 entries) at a
+// time, one quad ahead with the streaming hint, the quad's four neighbour positions are gathered together, and
+// every entry's terms are evaluated and masked (an exact 0.0 outside r_c and for the row's padding). Own and
+// reverse entries take one form: the reverse pair's -F(j, i) dx(j, i) equals +F dx(i, j), since min_image is
+// odd (round() and the |d| <= L/4 shortcut are symmetric) and IEEE subtraction antisymmetric, so each sum sees
+// the reference's nonzero terms in the reference's order; a masked 0.0 leaves a sum unchanged because a sum
+// that starts at +0.0 never becomes -0.0.
+__global__ void __launch_bounds__(128) k_force_fp64_quads(const double4* __restrict__ pos, int n, Box box, LJ lj,
+                                                          const uint32_t* __restrict__ rows, int cap,
+                                                          const int2* __restrict__ counts, double* __restrict__ force,
+                                                          unsigned long long* __restrict__ inside,
+                                                          double* __restrict__ kick_vel, const double* __restrict__ mass,
+                                                          double half_dt, const long long* __restrict__ half_off,
+                                                          double2* __restrict__ pair_ew) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long ins = 0;
+    if (i < n) {
+        const double4 pi = pos[i];
+        const int2 c = counts[i];
+        const int m = c.x + c.y;
+        const int quads = (m + 3) >> 2;
+        const long long pb = pair_ew ? half_off[i] : 0;
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        const uint4* rq = reinterpret_cast<const uint4*>(rows) + static_cast<size_t>(i >> 5) * (cap >> 2) * 32 + (i & 31);
+        uint4 nq = make_uint4(0, 0, 0, 0);
+        if (quads > 0) nq = __ldcs(rq);
+        for (int q = 0; q < quads; ++q) {
+            const uint4 eq = nq;
+            if (q + 1 < quads) nq = __ldcs(rq + 32 * (q + 1));
+            const uint32_t ent[4] = {eq.x, eq.y, eq.z, eq.w};
+            double4 pj[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) pj[u] = pos[4 * q + u < m ? static_cast<int>(ent[u] & kIndexMask) : 0];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int sl = 4 * q + u;
+                const double dx = min_image(dsub(pi.x, pj[u].x), box);
+                const double dy = min_image(dsub(pi.y, pj[u].y), box);
+                const double dz = min_image(dsub(pi.z, pj[u].z), box);
+                const double r2 = norm2(dx, dy, dz);
+                const bool in = sl < m && r2 < lj.rc2;
+                double f, e;
+                pair_terms(in ? r2 : 1.0, lj, f, e);
+                fx = dadd(fx, in ? dmul(f, dx) : 0.0);
+                fy = dadd(fy, in ? dmul(f, dy) : 0.0);
+                fz = dadd(fz, in ? dmul(f, dz) : 0.0);
+                if (sl < c.x) {
+                    ins += in ? 1u : 0u;
+                    if (pair_ew) store_pair_ew(pair_ew, pb + sl, in, f, e, r2);
+                }
+            }
+        }
+        const double F[3] = {fx, fy, fz};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const size_t o = static_cast<size_t>(k) * n + i;
+            force[o] = F[k];
+            if (kick_vel) kick_vel[o] = dadd(kick_vel[o], ddiv(dmul(half_dt, F[k]), mass[i]));
+        }
+    }
+    ins = warp_sum_u64(ins);
+    if ((threadIdx.x & 31) == 0 && ins) atomicAdd(inside, ins);
+}
+
 constexpr int kEnergyWarps = 4;  // warps per block of the blocked kinetic-energy sums
 
 // The inner loop of deterministicSum (include/Parallel.hpp:43-46) over the (pairEnergy, pairVirial) array the

@@ -365,9 +365,9 @@ class NeighbourList:
         return self._info()[2]
 
     def set_force_variant(self, precision: int, variant: int):
-        """-1 autotunes the list force kernel; 0 pins global gathers; 1 pins the shared-memory tile kernel; for
-        the float modes 2 pins prefetching global gathers, 3 the same with capped registers and 4 the same on a
-        resident grid. Every variant gives the same bits."""
+        """-1 autotunes the list force kernel; 0 pins global gathers; 1 pins the shared-memory tile kernel; 2 pins
+        prefetching global gathers (FP64: branch-free quads); for the float modes 3 pins variant 2 with capped
+        registers and 4 the same on a resident grid. Every variant gives the same bits."""
         _check(LIB.md_nlist_set_force_variant(self.h, precision, variant))
 
     def force_variant(self, precision: int) -> int:

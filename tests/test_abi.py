@@ -72,13 +72,13 @@ def test_argument_errors_are_reported():
     assert e.value.name == "MD_ERR_INVALID"
     with pytest.raises(mdgpu.MDError):
         mdgpu.RadialDistribution(1.0, 0)
-    # force variants: 0-4 for the float modes, 0-1 for FP64, 0 for FX64, -1 autotunes
+    # force variants: 0-4 for the float modes, 0-2 for FP64, 0 for FX64, -1 autotunes
     nl = mdgpu.NeighbourList(2.5, 0.3)
-    for prec, v in ((mdgpu.PREC_FP32FX, 5), (mdgpu.PREC_FP32, -2), (mdgpu.PREC_FP64, 2), (mdgpu.PREC_FX64, 1)):
+    for prec, v in ((mdgpu.PREC_FP32FX, 5), (mdgpu.PREC_FP32, -2), (mdgpu.PREC_FP64, 3), (mdgpu.PREC_FX64, 1)):
         with pytest.raises(mdgpu.MDError) as e:
             nl.set_force_variant(prec, v)
         assert e.value.name == "MD_ERR_INVALID"
-    for prec, v in ((mdgpu.PREC_FP32FX, 4), (mdgpu.PREC_FP32, 3), (mdgpu.PREC_FP64, 1), (mdgpu.PREC_FX64, 0),
+    for prec, v in ((mdgpu.PREC_FP32FX, 4), (mdgpu.PREC_FP32, 3), (mdgpu.PREC_FP64, 2), (mdgpu.PREC_FX64, 0),
                     (mdgpu.PREC_FP32FX, -1)):
         nl.set_force_variant(prec, v)
 
