@@ -343,7 +343,8 @@ def adjoint_workload(md, a, device: int) -> dict:
     s = md.fcc_system(20, 0.8442, 1.0, seed=42, device=device)
     d = s.download()
     eng = md.Adjoint(d["pos"], s.box, d["vel"], steps=a.adjoint_steps, checkpoint_every=20, device=device)
-    eng.forward()
+    eng.forward()  # untimed forward and backward: module loading and first-use allocations stay out of the timings
+    eng.backward(1.0, 0.0)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     mu, mp = eng.forward()
