@@ -549,7 +549,8 @@ def run_gpu_arm(a):
                          "frac": achieved / peak, "traffic": None if tpa is None else tpa * n,
                          "kernel": {"fp64": "k_force_fp64", "fx64": "k_force_fx64_rows"}.get(a.precision, "k_force_fp32"),
                          "force_variant": {0: "global gathers", 1: "shared-memory tiles",
-                                           2: "global gathers, rows prefetched",
+                                           2: ("global gathers, branch-free quads" if a.precision == "fp64"
+                                               else "global gathers, rows prefetched"),
                                            3: "global gathers, rows prefetched, registers capped",
                                            4: "global gathers, rows prefetched, resident grid"}.get(variant, str(variant)),
                          "kernel_ms": kernel_s * 1e3,
