@@ -464,33 +464,36 @@ __global__ void __launch_bounds__(kTile)
         const int a = d.off + i;
         const double4 pi = pos[a];
         const int2 c = counts[a];
+        const int m = c.x + c.y;
+        const int quads = (m + 3) >> 2;
         double fx = 0.0, fy = 0.0, fz = 0.0;
-        for (int s = 0; s < c.x; ++s) {
-            const double4 pj = pos[rows[row_index(a, s, cap)] & kIndexMask];
-            const double dx = min_image(dsub(pi.x, pj.x), d.box);
-            const double dy = min_image(dsub(pi.y, pj.y), d.box);
-            const double dz = min_image(dsub(pi.z, pj.z), d.box);
-            const double r2 = norm2(dx, dy, dz);
-            if (!(r2 < lj.rc2)) continue;
-            double f, e;
-            pair_terms(r2, lj, f, e);
-            fx = dadd(fx, dmul(f, dx));
-            fy = dadd(fy, dmul(f, dy));
-            fz = dadd(fz, dmul(f, dz));
-            ++ins;
-        }
-        for (int s = c.x; s < c.x + c.y; ++s) {
-            const double4 pj = pos[rows[row_index(a, s, cap)] & kIndexMask];
-            const double dx = min_image(dsub(pj.x, pi.x), d.box);
-            const double dy = min_image(dsub(pj.y, pi.y), d.box);
-            const double dz = min_image(dsub(pj.z, pi.z), d.box);
-            const double r2 = norm2(dx, dy, dz);
-            if (!(r2 < lj.rc2)) continue;
-            double f, e;
-            pair_terms(r2, lj, f, e);
-            fx = dsub(fx, dmul(f, dx));
-            fy = dsub(fy, dmul(f, dy));
-            fz = dsub(fz, dmul(f, dz));
+        // k_force_fp64_quads' loop: a quad of row entries at a time, the next one in flight, every entry evaluated
+        // and masked, the reverse pairs in the own form (the same bits as the reference's two loops)
+        const uint4* rq = reinterpret_cast<const uint4*>(rows) + static_cast<size_t>(a >> 5) * (cap >> 2) * 32 + (a & 31);
+        uint4 nq = make_uint4(0, 0, 0, 0);
+        if (quads > 0) nq = __ldcs(rq);
+        for (int q = 0; q < quads; ++q) {
+            const uint4 eq = nq;
+            if (q + 1 < quads) nq = __ldcs(rq + 32 * (q + 1));
+            const uint32_t ent[4] = {eq.x, eq.y, eq.z, eq.w};
+            double4 pj[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) pj[u] = pos[4 * q + u < m ? static_cast<int>(ent[u] & kIndexMask) : a];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int sl = 4 * q + u;
+                const double dx = min_image(dsub(pi.x, pj[u].x), d.box);
+                const double dy = min_image(dsub(pi.y, pj[u].y), d.box);
+                const double dz = min_image(dsub(pi.z, pj[u].z), d.box);
+                const double r2 = norm2(dx, dy, dz);
+                const bool in = sl < m && r2 < lj.rc2;
+                double f, e;
+                pair_terms(in ? r2 : 1.0, lj, f, e);
+                fx = dadd(fx, in ? dmul(f, dx) : 0.0);
+                fy = dadd(fy, in ? dmul(f, dy) : 0.0);
+                fz = dadd(fz, in ? dmul(f, dz) : 0.0);
+                ins += (in && sl < c.x) ? 1u : 0u;
+            }
         }
         const double F[3] = {fx, fy, fz};
 #pragma unroll
