@@ -220,13 +220,11 @@ def replica_throughput(world: int, n_atoms: int, steps: int, max_ms: float) -> f
 # ---- GPU arm ------------------------------------------------------------------------------------------------
 
 def measured_peak():
-    for path in (os.path.join(ROOT, "MEASURED_PEAKS.json"), "/root/repo/MEASURED_PEAKS.json"):
-        try:
-            with open(path) as f:
-                return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, copy)"
-        except (OSError, KeyError, ValueError):
-            continue
-    return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, copy)"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
 
 
 def ncu_traffic_per_atom():
