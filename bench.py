@@ -53,10 +53,13 @@ def args_parse():
     p.add_argument("--temperature", type=float, default=0.71)
     p.add_argument("--equil", type=int, default=200)
     p.add_argument("--precision", choices=list(PRECISIONS), default="fp32fx")
-    p.add_argument("--fp64-steps", type=int, default=100, help="steps of the FP64 comparison run (0: skip)")
+    p.add_argument("--fp64-steps", type=int, default=None,
+                   help="steps of the FP64 comparison run from the headline's starting state (default: --steps; 0: skip)")
     p.add_argument("--side-steps", type=int, default=300,
                    help="steps of the runs of the other float precisions on the same state (0: skip)")
-    p.add_argument("--cpu-steps", type=int, default=3, help="reference steps in the cpu_baseline sample (0: skip)")
+    p.add_argument("--cpu-steps", type=int, default=None,
+                   help="timed reference steps of the CPU samples (default: --steps, capped at 200; 0: skip the "
+                        "cpu_baseline leg); the untimed steps are --warmup, capped at 20")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--sweep", choices=["precision"], default=None,
                    help="instead of the headline line: the N=256,000 precision sweep over densities {0.5, 0.8442, 1.0} "
@@ -83,15 +86,29 @@ def workload(a) -> dict:
 
 # ---- reference CPU path --------------------------------------------------------------------------------------
 
+REF_MAX_STEPS = 200  # cap of the CPU samples (about 0.6 s per 4M-atom step on 16 host threads)
+REF_MAX_WARMUP = 20
+
+
+def cpu_sample_shape(a) -> tuple[int, int]:
+    """Timed and untimed steps of a CPU sample: the run's own --steps/--warmup, capped so the sample stays
+    within a few minutes. Both CPU legs (the GPU arm's cpu_baseline and the reference arm) use this."""
+    steps = a.cpu_steps if a.cpu_steps is not None else a.steps
+    return max(1, min(steps, REF_MAX_STEPS)), min(a.warmup, REF_MAX_WARMUP)
+
+
 def reference_sample(a, steps: int, warmup: int) -> dict:
-    """Time the reference's OpenMP path (oracle/_ref, compiled from its own sources) on all host cores: the
-    same FCC start, list build and list forces, then `warmup` untimed and `steps` timed NVE steps (default
-    force path, as md_sim runs without --deterministic)."""
-    from oracle.oracle import REF_SO, Oracle, Reference, RForceField, RNeighbourList
+    """Time the reference's OpenMP path on all host cores: the same 4M-atom FCC start, list build and list
+    forces, then `warmup` untimed and `steps` timed NVE steps of the default (non-deterministic) force path, as
+    md_sim runs without --deterministic, with list rebuilds at their natural rate inside the timed steps. The
+    library timed is the reference's unmodified sources built with its release flags (oracle/_ref/
+    libmdref_stock_*.so); the strict parity build is used only where those were not built."""
+    from oracle.oracle import Oracle, Reference, RForceField, RNeighbourList, stock_reference_path
 
     threads = os.cpu_count() or 1
-    if os.path.exists(REF_SO):
-        r = Reference()
+    path, build = stock_reference_path()
+    if os.path.exists(path):
+        r = Reference(path)
         r.set_threads(threads)
         t0 = time.perf_counter()
         s = r.fcc_system(a.cells, a.density, a.temperature, 42)
@@ -109,6 +126,7 @@ def reference_sample(a, steps: int, warmup: int) -> dict:
         kind, cores, rebuilds = "reference", r.max_threads(), nl.rebuilds - rb0
     else:  # the oracle's serial restatement, when the reference could not be built on this machine
         from oracle.oracle import MODE_DEFAULT, OForceField, ONeighbourList
+        build = "the oracle's serial restatement"
         o = Oracle()
         t0 = time.perf_counter()
         s = o.fcc_system(a.cells, a.density, a.temperature, 42)
@@ -128,16 +146,15 @@ def reference_sample(a, steps: int, warmup: int) -> dict:
     n = 4 * a.cells ** 3
     return {"value": n * steps / dt, "unit": "atom-steps/s", "cores": cores, "kind": kind,
             "sample": f"{steps} timed NVE steps (after {warmup} untimed) of the same {n}-atom FCC start, "
-                      f"list start, FP64 default force path, {rebuilds} list rebuilds inside the sample; "
-                      f"setup {setup:.1f} s untimed",
-            "ms_per_step": 1e3 * dt / steps, "steps": steps}
+                      f"list start, FP64 default force path, {rebuilds} list rebuilds inside the timed steps; "
+                      f"{build}; setup {setup:.1f} s untimed",
+            "ms_per_step": 1e3 * dt / steps, "steps": steps, "warmup": warmup, "rebuilds": rebuilds}
 
 
 def run_reference_arm(a):
     if int(os.environ.get("RANK", "0")) != 0:
         return  # rank 0 alone runs the CPU reference
-    steps = max(1, min(a.steps, 5))
-    warm = min(a.warmup, 2)
+    steps, warm = cpu_sample_shape(a)
     cb = reference_sample(a, steps, warm)
     line = {"metric": METRIC, "value": cb["value"], "unit": "atom-steps/s", "impl": "reference",
             "n_gpus": a.gpus, "steps": steps, "warmup": warm, "ms_per_step": cb["ms_per_step"],
@@ -333,9 +350,11 @@ def replica_workload(md, a, device: int) -> dict:
 
 def adjoint_workload(md, a, device: int) -> dict:
     """The differentiation workload: N = 32,000 (FCC 20^3 x 4), density 0.8442, T* = 1.0, `a.adjoint_steps` NVE
-    steps of dt = 0.005, checkpoints every 20; timings of forward and backward, and the gradient of mean U with
-    respect to epsilon against central differences at h = 1e-4 (the cutoff's force jump enters the stencil),
-    1e-7 and 1e-8."""
+    steps of dt = 0.005, checkpoints every 20; timings of forward and backward, and the gradients of mean U with
+    respect to epsilon, sigma and the initial positions (along one random unit direction) against central
+    differences at h = 1e-4 (the workload's nominal step: the cutoff's force jump enters the stencil), 1e-7 and
+    1e-8 (relative error per step size)."""
+    import numpy as np
     import torch
 
     s = md.fcc_system(20, 0.8442, 1.0, seed=42, device=device)
@@ -349,19 +368,33 @@ def adjoint_workload(md, a, device: int) -> dict:
     t1 = time.perf_counter()
     g = eng.backward(1.0, 0.0)
     t2 = time.perf_counter()
+    pos0 = d["pos"]
+    rng = np.random.default_rng(3)
+    u = np.zeros_like(pos0)
+    u[:, :3] = rng.standard_normal((len(pos0), 3))
+    u /= np.linalg.norm(u)
 
-    def J(eps):
-        eng.set_parameters(eps, 1.0)
+    def J(eps=1.0, sig=1.0, pos=pos0):
+        eng.set_parameters(eps, sig)
+        eng.set_state(pos=pos)
         return eng.forward()[0]
 
-    fd = {h: (J(1.0 + h) - J(1.0 - h)) / (2 * h) for h in (1e-4, 1e-7, 1e-8)}
-    eng.set_parameters(1.0, 1.0)
+    checks = {"epsilon": (g["d_epsilon"], lambda h: J(eps=1.0 + h)),
+              "sigma": (g["d_sigma"], lambda h: J(sig=1.0 + h)),
+              "positions": (float((g["d_pos"].T * u[:, :3]).sum()), lambda h: J(pos=pos0 + h * u))}
+    fd = {}
+    for name, (adj, f) in checks.items():
+        fd[name] = {str(h): abs((f(h) - f(-h)) / (2 * h) - adj) / abs(adj) for h in (1e-4, 1e-7, 1e-8)}
+    J()
     n = s.n
     return {"workload": f"N={n} FCC 20^3x4, rho=0.8442, T=1.0, {a.adjoint_steps} NVE steps, checkpoints every 20",
             "mean_pe": mu, "mean_pressure": mp, "forward_s": t1 - t0, "backward_s": t2 - t1,
             "forward_atom_steps_per_s": n * a.adjoint_steps / (t1 - t0),
             "d_mean_pe_d_epsilon": g["d_epsilon"], "d_mean_pe_d_sigma": g["d_sigma"],
-            "fd_rel_err_epsilon": {str(h): abs(v - g["d_epsilon"]) / abs(g["d_epsilon"]) for h, v in fd.items()},
+            "fd_rel_err": fd,
+            "fd_note": "central differences of mean U; h = 1e-4 puts pairs across the cutoff's force jump inside the "
+                       "stencil, so the clean figures are the smaller h (the GPU gradients equal the FP64 CPU "
+                       "adjoint's bit for bit)",
             "rebuilds": eng.info()["rebuilds"]}
 
 
@@ -399,6 +432,8 @@ def run_gpu_arm(a):
     if a.warmup:
         integ.run(s, ff, nl, a.warmup, first_step=a.equil + 1)
 
+    # the state the timed steps start from: the FP64 and other-precision runs below start from it too
+    start = s.download() if rank == 0 and (a.fp64_steps != 0 or a.side_steps) else None
     stream = torch.cuda.ExternalStream(s.stream)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if dist:
@@ -430,20 +465,20 @@ def run_gpu_arm(a):
     e0 = pe[0] + ke[0]
     drift = float(np.abs((pe + ke - e0) / e0).max())
 
-    # The FP64 path (bit-identical to the reference's deterministic mode) and the other float precisions on
-    # copies of the same state
+    # The FP64 path (bit-identical to the reference's deterministic mode) and the other precisions, each from the
+    # state the timed steps started from: list build, forces (the first force call tunes the kernel), then the
+    # steps timed with CUDA events and their energy drift, max |E_k - E_1| / |E_1| as for the headline run
     def side_run(precision: int, steps: int) -> dict:
-        st = s.download()
-        s2 = md.System.from_arrays(st["pos"], s.box, vel=st["vel"], force=st["force"], device=local)
+        s2 = md.System.from_arrays(start["pos"], s.box, vel=start["vel"], force=start["force"], device=local)
         nl2 = md.NeighbourList(2.5, 0.3)
         nl2.build(s2)
         ff2 = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=precision)
         ff2.compute_forces(s2, nl2)
-        integ.run(s2, ff2, nl2, 5)
         st2 = torch.cuda.ExternalStream(s2.stream)
         e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s2.synchronize()
         s2.profile(True)
+        rb = nl2.rebuild_count
         e0_.record(st2)
         pe2, ke2, _ = integ.run(s2, ff2, nl2, steps)
         e1_.record(st2)
@@ -451,10 +486,12 @@ def run_gpu_arm(a):
         ms2 = e0_.elapsed_time(e1_)
         f_ms, f_n = s2.profile_read()
         return {"value": n * steps / (ms2 / 1e3), "steps": steps, "ms_per_step": ms2 / steps,
-                "force_kernel_ms": f_ms / max(f_n, 1),
-                "max_drift": float(np.abs((pe2 + ke2 - pe2[0] - ke2[0]) / (pe2[0] + ke2[0])).max())}
+                "force_kernel_ms": f_ms / max(f_n, 1), "rebuilds": nl2.rebuild_count - rb,
+                "max_drift": float(np.abs((pe2 + ke2 - pe2[0] - ke2[0]) / (pe2[0] + ke2[0])).max()),
+                "start": "the state the headline's timed steps started from"}
 
-    fp64 = side_run(md.PREC_FP64, a.fp64_steps) if a.fp64_steps and rank == 0 else None
+    fp64_steps = a.steps if a.fp64_steps is None else a.fp64_steps
+    fp64 = side_run(md.PREC_FP64, fp64_steps) if fp64_steps and rank == 0 else None
     others = {}
     if a.side_steps and rank == 0:
         for name in ("fp32fx", "fx64", "fp32"):
@@ -507,8 +544,8 @@ def run_gpu_arm(a):
     adjoint = adjoint_workload(md, a, local) if rank == 0 and a.adjoint_steps > 0 else None
 
     cpu = None
-    if rank == 0 and world == 1 and a.cpu_steps > 0:
-        cb = reference_sample(a, a.cpu_steps, 1)
+    if rank == 0 and world == 1 and a.cpu_steps != 0:
+        cb = reference_sample(a, *cpu_sample_shape(a))
         cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
     if rank != 0:

@@ -102,10 +102,14 @@ md_status md_initialize_velocities(md_system* s, double temperature, uint32_t se
  * 1024-particle blocked order). Work is queued on `stream` (a cudaStream_t; NULL = legacy default stream)
  * and the call returns without waiting. Scratch lives in a fixed 256 KB device array that every GPU loading
  * the library keeps until exit; n above 16,777,216 is rejected with MD_ERR_INVALID. The first call on a
- * device looks that array up on the current device (cudaGetSymbolAddress), so make the first call on each
- * device before any stream capture. All calls share the one array: calls that overlap on the GPU (on
- * different streams, or from different host threads) race and must be serialised by the caller. The
- * current device must be the one holding the pointers. No allocating call is made. */
+ * device (and the first after a device reset, which gives the device a new context) looks that array up on
+ * the current device (cudaGetSymbolAddress), so make the first call on each device before any stream
+ * capture. That first call may also be what loads the library's device code (CUDA loads modules lazily by
+ * default), and the driver backs the loaded code and the array with device memory; a host that must see no
+ * allocation after start-up makes one warm-up call then, or runs with CUDA_MODULE_LOADING=EAGER. Later calls
+ * make no allocating call (no cudaMalloc, cudaFree or allocating library routine). All calls share the one
+ * array: calls that overlap on the GPU (on different streams, or from different host threads) race and must
+ * be serialised by the caller. The current device must be the one holding the pointers. */
 md_status md_kinetic_energy_noalloc(const double* vel3, const double* mass, int64_t n, double* out, void* stream);
 
 /* writeXyzFrame's data (src/Trajectory.cpp:4-25) in id order: out6[6 id + k] = (x, y, z, vx, vy, vz)[k] of

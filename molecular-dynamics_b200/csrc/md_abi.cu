@@ -1484,20 +1484,49 @@ constexpr int64_t kNoAllocMaxBlocks = 16384;  // 1024-particle blocks: up to 16,
 static __device__ __align__(256) double2 g_noalloc_ke_blocks[kNoAllocMaxBlocks + 1];
 
 // Host code must not take g_noalloc_ke_blocks' address directly (it names a host-side shadow): the device
-// address comes from cudaGetSymbolAddress, once per device, with that device current.
+// address comes from cudaGetSymbolAddress, once per device, with that device current. The address is kept
+// with the context it was looked up in: after a device reset the primary context is a new one, the module is
+// loaded again at another address, and the address is looked up again.
 constexpr int kNoAllocMaxDevices = 64;
-double2* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+struct NoAllocScratch {
+    void* context = nullptr;  // CUcontext current when ptr was looked up
+    double2* ptr = nullptr;
+};
+NoAllocScratch g_noalloc[kNoAllocMaxDevices] = {};
 std::mutex g_noalloc_mutex;
+
+// The calling thread's current CUcontext, through the runtime's driver entry point (no link against libcuda)
+md_status current_context(void** ctx) {
+    using GetCurrent = int (*)(void**);
+    static GetCurrent get = nullptr;
+    if (!get) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        MD_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess) return fail(MD_ERR_CUDA, "cuCtxGetCurrent is unavailable");
+        get = reinterpret_cast<GetCurrent>(fn);
+    }
+    *ctx = nullptr;
+    if (get(ctx) != 0) return fail(MD_ERR_CUDA, "cuCtxGetCurrent failed");
+    return MD_OK;
+}
 
 md_status noalloc_scratch(int device, double2** out) {
     if (device < 0 || device >= kNoAllocMaxDevices) return fail(MD_ERR_INVALID, "device index out of range");
+    // NULL until the runtime has made the device's primary context current on this thread, which the
+    // symbol lookup below does
+    void* ctx = nullptr;
+    MD_TRY(current_context(&ctx));
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[device]) {
+    NoAllocScratch& e = g_noalloc[device];
+    if (!e.ptr || !ctx || e.context != ctx) {
         void* p = nullptr;
         MD_CUDA(cudaGetSymbolAddress(&p, g_noalloc_ke_blocks));
-        g_noalloc_ptr[device] = static_cast<double2*>(p);
+        MD_TRY(current_context(&ctx));
+        e.ptr = static_cast<double2*>(p);
+        e.context = ctx;
     }
-    *out = g_noalloc_ptr[device];
+    *out = e.ptr;
     return MD_OK;
 }
 

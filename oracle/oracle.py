@@ -4,7 +4,8 @@ ctypes access to the two CPU libraries that oracle/Makefile builds:
 
 * ``Oracle``: liboracle.so, the serial restatement of the reference's hot path (oracle/md_oracle.cpp);
 * ``Reference``: oracle/_ref/libmdref.so, the reference's own sources compiled unmodified, driven through
-  oracle/ref_harness.cpp.
+  oracle/ref_harness.cpp (strict IEEE build, for parity); ``stock_reference_path()`` names the same sources built
+  with the reference's release flags, for timing.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU legs import this module.
 """
@@ -20,6 +21,29 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmdref.so")
 REF_MD_SIM = os.path.join(HERE, "_ref", "md_sim")
+REF_STOCK = {"v4": os.path.join(HERE, "_ref", "libmdref_stock_v4.so"),
+             "v3": os.path.join(HERE, "_ref", "libmdref_stock_v3.so")}
+_V4_FLAGS = {"avx512f", "avx512dq", "avx512cd", "avx512bw", "avx512vl"}
+
+
+def stock_reference_path() -> tuple[str, str]:
+    """The reference built with its release flags (-O3, FMA contraction on; CMakeLists.txt:12) for the ISA level
+    this host runs -- x86-64-v4 (AVX-512) when /proc/cpuinfo lists its flags, else x86-64-v3 -- standing in for
+    -march=native. Falls back to the strict parity build when neither was built. Returns (path, description)."""
+    flags = set()
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    break
+    except OSError:
+        pass
+    level = "v4" if _V4_FLAGS <= flags else "v3"
+    for lv in ([level, "v3"] if level == "v4" else ["v3"]):
+        if os.path.exists(REF_STOCK[lv]):
+            return REF_STOCK[lv], f"reference sources, release flags (-O3, FMA contraction on, -march=x86-64-{lv})"
+    return REF_SO, "reference sources, strict parity build (-O3 -march=x86-64-v3 -ffp-contract=off)"
 
 _P = C.c_void_p
 _D = C.c_double

@@ -242,6 +242,33 @@ TEST(ForceField, MixedPrecisionMatchesDoubleAndConservesEnergy) {
     CHECK(drift < 3e-4);
 }
 
+// Precision::FixedDouble (exact fixed-point separations, double pair terms): every particle's force within 1e-6
+// of the rms force of the double path, the energy within 1e-9
+TEST(ForceField, FixedDoublePrecisionMatchesDouble) {
+    System s = makeLiquid(8);
+    LennardJonesForceField ff(1.0, 1.0, cutOff);
+    NeighbourList list(cutOff, skin);
+    list.build(s);
+    const double e = ff.computeForces(s, list);
+    std::vector<std::array<double, 3>> ref;
+    double rms = 0.0;
+    for (std::size_t i = 0; i < s.size(); ++i) {
+        ref.push_back(s.forceOf(i));
+        for (double f : ref.back()) rms += f * f;
+    }
+    rms = std::sqrt(rms / static_cast<double>(s.size()));
+    ff.setPrecision(LennardJonesForceField::Precision::FixedDouble);
+    const double fe = ff.computeForces(s, list);
+    CHECK_NEAR(fe, e, 1e-9 * std::abs(e));
+    double worst = 0.0;
+    for (std::size_t i = 0; i < ref.size(); ++i) {
+        double d2 = 0.0;
+        for (int k = 0; k < 3; ++k) d2 += (s.forceOf(i)[k] - ref[i][k]) * (s.forceOf(i)[k] - ref[i][k]);
+        worst = std::max(worst, std::sqrt(d2));
+    }
+    CHECK(worst < 1e-6 * rms);
+}
+
 // ---- tests/test_neighbourlist.cpp --------------------------------------------------------------------------
 
 TEST(NeighbourList, ContentsFallbackRebuildAndErrors) {

@@ -77,9 +77,12 @@ def test_gpu_adjoint_against_central_differences(md, oracle, cells, steps, param
                   "positions": (float((g["d_pos"].T * dp[:, :3]).sum()), lambda h: J(pos=st.pos + h * dp))}
         for name in params:
             adj, f = checks[name]
-            errs = {h: abs(central(f, h) - adj) / abs(adj) for h in hs}
+            # h = 1e-4 (the workload's nominal step) is reported beside the clean step sizes and not asserted on;
+            # the assertion takes the best of the clean step sizes listed in the parametrisation
+            errs = {h: abs(central(f, h) - adj) / abs(adj) for h in (1e-4, *hs)}
             print(cells, name, g_pe, g_p, adj, errs)
-            assert min(errs.values()) < 1e-6, (name, adj, errs)
+            best = min(hs, key=lambda h: errs[h])
+            assert errs[best] < 1e-6, (name, adj, errs)
     gpu.set_parameters(1.0, 1.0)
     gpu.set_state(pos=st.pos)
 

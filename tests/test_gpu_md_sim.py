@@ -83,3 +83,18 @@ def test_md_sim_reordered_paths_within_tolerance(golden, tmp_path, case, rtol):
     assert (err <= rtol + 1e-8).all(), err
     assert abs(float(out["result"]["mean_T"]) - float(g["result"]["mean_T"])) <= 1e-5
     assert out["result"]["rebuilds"] == g["result"]["rebuilds"]
+
+
+# --precision fx64 (exact fixed-point separations, double pair terms, 64-bit fixed-point sums): the per-particle
+# force error against FP64 is about 2e-7 of the rms force, so the observables of the reference's own
+# --deterministic run on the same command line stay within 2e-6 of their largest magnitude over 400 steps
+def test_md_sim_fx64_within_bound_of_reference_deterministic(golden, tmp_path):
+    g = golden["nve_rescale"]
+    out = run_md_sim([*g["args"], "--precision", "fx64"], str(tmp_path))
+    ref, got = csv_columns(g["files"]["csv"]), csv_columns(out["files"]["csv"])
+    assert got.shape == ref.shape
+    assert np.array_equal(got[:, 0], ref[:, 0])
+    scale = np.abs(ref[:, 2:7]).max(axis=0)
+    err = np.abs(got[:, 2:7] - ref[:, 2:7]).max(axis=0) / scale
+    assert (err <= 2e-6).all(), err
+    assert out["result"]["rebuilds"] == g["result"]["rebuilds"]
