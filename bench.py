@@ -39,7 +39,8 @@ for _p in (ROOT, PKG):
 METRIC = "atom-steps/s at N=4M, FP32+fixed-pt vs FP64 GPU at <=1e-6 rel force err; %roofline"
 FALLBACK_HBM_GBS = 6650.0
 # precision name -> (md_precision value, arithmetic of the pair path)
-PRECISIONS = {"fp32fx": (1, "f32+i64"), "fp32": (2, "f32"), "fp64": (0, "f64"), "fx64": (3, "i32+f64+i64")}
+PRECISIONS = {"fp32fx": (1, "f32+i64"), "fp32": (2, "f32"), "fp64": (0, "f64"), "fx64": (3, "i32+f64+i64"),
+              "fx32": (4, "i32+f32+i64 (f64 for close pairs)")}
 
 
 def args_parse():
@@ -263,7 +264,7 @@ def force_errors(md, s, nl) -> dict:
     w64 = ff64.virial
     f64 = s.forces()
     out = {}
-    for name in ("fp32fx", "fp32", "fx64"):
+    for name in ("fp32fx", "fp32", "fx64", "fx32"):
         ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=PRECISIONS[name][0])
         pe = ff.compute_forces(s, nl)
         f = s.forces()
@@ -494,7 +495,7 @@ def run_gpu_arm(a):
     fp64 = side_run(md.PREC_FP64, fp64_steps) if fp64_steps and rank == 0 else None
     others = {}
     if a.side_steps and rank == 0:
-        for name in ("fp32fx", "fx64", "fp32"):
+        for name in ("fx32", "fp32fx", "fx64", "fp32"):
             if name != a.precision:
                 others[name] = side_run(PRECISIONS[name][0], a.side_steps)
 
@@ -561,7 +562,7 @@ def run_gpu_arm(a):
     # records for the ordered energy sums.
     own = 32 if a.precision == "fp64" else 16
     bytes_per_atom = own + 24 + 4 * 2 * pairs / n + 56
-    if a.precision in ("fp32fx", "fp32"):
+    if a.precision in ("fp32fx", "fp32", "fx32", "fx64"):
         bytes_per_atom += 32 + 32 + 4 + 32 + 16
     if a.precision == "fp64":
         bytes_per_atom += 16 * pairs / n
@@ -582,7 +583,8 @@ def run_gpu_arm(a):
             "data": "synthetic", "config": workload(a),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None if tpa is None else tpa * n,
-                         "kernel": {"fp64": "k_force_fp64", "fx64": "k_force_fx64_rows"}.get(a.precision, "k_force_fp32"),
+                         "kernel": {"fp64": "k_force_fp64", "fx64": "k_force_fx64_rows",
+                                    "fx32": "k_force_fx32"}.get(a.precision, "k_force_fp32"),
                          "force_variant": {0: "global gathers", 1: "shared-memory tiles",
                                            2: ("global gathers, branch-free quads" if a.precision == "fp64"
                                                else "global gathers, rows prefetched"),
@@ -631,7 +633,7 @@ def precision_sweep(cells=40, densities=(0.5, 0.8442, 1.0), temperatures=(0.71, 
             start = s.download()
             vol = s.box ** 3
             runs = {}
-            for name in ("fp64", "fp32fx", "fp32", "fx64"):
+            for name in ("fp64", "fp32fx", "fp32", "fx64", "fx32"):
                 prec = PRECISIONS[name][0]
                 r = md.System.from_arrays(start["pos"], s.box, vel=start["vel"], force=start["force"], device=device)
                 rl = md.NeighbourList(2.5, 0.3)

@@ -39,8 +39,11 @@ typedef enum md_precision {
     MD_PREC_FP64 = 0,   /* double throughout, bit-identical to the reference's deterministic path */
     MD_PREC_FP32FX = 1, /* float pair arithmetic, 64-bit fixed-point force accumulation */
     MD_PREC_FP32 = 2,   /* float pair arithmetic, float accumulation */
-    MD_PREC_FX64 = 3    /* exact separations from 32-bit fixed-point frames, double pair terms, 64-bit
+    MD_PREC_FX64 = 3,   /* exact separations from 32-bit fixed-point frames, double pair terms, 64-bit
                            fixed-point accumulation */
+    MD_PREC_FX32 = 4    /* exact separations from 32-bit fixed-point frames; float pair terms for pairs that
+                           were at least 1.3 sigma + skin apart at the list build, double pair terms for the
+                           closer ones (about one in six); 64-bit fixed-point accumulation */
 } md_precision;
 
 typedef struct md_system md_system;         /* System (include/System.hpp:12) */
@@ -155,7 +158,9 @@ md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_c
  * available variant and keeps the fastest), 0 pins global gathers, 1 pins the shared-memory tile kernel (used
  * only while the list has tiles; FP64 and the float modes), 2 pins global gathers with the rows prefetched
  * (FP64: a quad of entries at a time, branch-free; float modes: a group of 8 ahead), 3 the float modes' variant 2
- * with registers capped for occupancy and 4 the same on a resident grid. Every variant gives the same bits. md_nlist_force_variant reports the variant in use (-1 until the first force call). */
+ * with registers capped for occupancy and 4 the same on a resident grid. MD_PREC_FX64 and MD_PREC_FX32 have one
+ * kernel each (variant 0). Every variant gives the same bits. md_nlist_force_variant reports the variant in use
+ * (-1 until the first force call). */
 md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant);
 md_status md_nlist_force_variant(const md_nlist* nl, int precision, int* variant);
 /* List build kernel: -1 uses the shared-memory tile build wherever the list has tiles, 0 pins one thread per
@@ -202,10 +207,17 @@ md_status md_step_list(md_system* s, md_forcefield* ff, md_nlist* nl, double dt,
 /* step(System&, const LennardJonesForceField&) with O(N^2) forces (src/Integrator.cpp:7-16). */
 md_status md_step_all_pairs(md_system* s, md_forcefield* ff, double dt, double* pe);
 
-/* Device-resident run of n_steps list steps with no host round trip per step (md_sim's loops,
- * src/main.cpp:219-304). Per step, in order: step_list; then the optional thermostat; then the optional
- * g(r) sample. Outputs (each NULL or n_steps long, host memory): pe[k] the step's PE, ke[k] the kinetic
- * energy after the thermostat, virial[k]. */
+/* n_steps list steps (md_sim's loops, src/main.cpp:219-304). Per step, in order: step_list; then the optional
+ * thermostat; then the optional g(r) sample. Outputs (each NULL or n_steps long, host memory): pe[k] the step's
+ * PE, ke[k] the kinetic energy after the thermostat, virial[k].
+ * The float precisions on a list with shared-memory tiles run as CUDA graphs of up to md_system_set_graph's
+ * chunk length (64 steps by default): every step, the thermostat and the g(r) sample included, is in the graph,
+ * and a list rebuild is decided on the device (a conditional node runs the rebuild when the half-skin test of the
+ * step's drift flagged a particle), so the host waits once per chunk. A rebuild that outgrows the row capacity or
+ * the recorded shared-memory tile makes the library run that chunk again on the host path from the chunk's
+ * starting state, growing what it must; results are the same bits either way. MD_PREC_FP64 (whose ordered
+ * energy sums need the pair count after each rebuild on the host), small boxes and lists pinned to the global
+ * build take the host-driven loop, which reads the half-skin flag after each drift. */
 typedef struct md_run_options {
     int thermostat;             /* 0 none (NVE), 1 rescale, 2 Bussi */
     int rescale_every;          /* rescale when (first_step + k) % rescale_every == 0 */
@@ -222,6 +234,19 @@ typedef struct md_run_options {
 } md_run_options;
 md_status md_run(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
                  const md_run_options* opts, double* pe, double* ke, double* virial);
+/* Capture and instantiate the graphs md_run would launch for the same arguments, without running a step (graph
+ * set-up stays out of a timed run). record: bit 0 when pe or virial will be requested, bit 1 when ke will. */
+md_status md_run_prepare(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
+                         const md_run_options* opts, int record);
+/* md_run's graph chunk length (1..1024 steps; 0 runs every step from the host) and test flags:
+ * MD_GRAPH_EXACT_TILES records the host's shared-memory tile bound in the graphs without headroom, so that
+ * rebuilds on the device outgrow it and the chunk reruns on the host path (for tests of that path). Drops the
+ * system's cached graphs. */
+#define MD_GRAPH_EXACT_TILES 1
+md_status md_system_set_graph(md_system* s, int chunk_steps, int flags);
+/* Graph chunk length, graphs cached, chunk graphs launched and chunks rerun on the host path. Any may be NULL. */
+md_status md_system_graph_info(const md_system* s, int* chunk_steps, uint64_t* graphs, uint64_t* launches,
+                               uint64_t* recoveries);
 
 /* ---- RadialDistribution: include/RadialDistribution.hpp:10-20, src/RadialDistribution.cpp ----------- */
 md_status md_rdf_create(double r_max, int bins, md_rdf** out);
@@ -271,6 +296,17 @@ md_status md_batch_stream(md_batch* b, void** stream);
 /* n_steps steps of every replica. With energy_every = k, row s of the records (replica r at [s * replicas + r])
  * is step (s + 1) k of this run; arrays hold n_steps / k rows each and may be NULL. */
 md_status md_batch_run(md_batch* b, int64_t n_steps, double* pe, double* virial, double* ke);
+/* md_batch_run that also records each sampled step's inside-cutoff pair count (getInsidePairs,
+ * include/Forcefield.hpp:26-29) into inside (same layout; NULL to skip): the count that converts the shifted
+ * potential energy to the unshifted one, as bench/validate.py:114-120 of the reference does. */
+md_status md_batch_run_records(md_batch* b, int64_t n_steps, double* pe, double* virial, double* ke, double* inside);
+/* Change the thermostat between runs (a protocol of phases, e.g. bench/validate.py:96-111's melt, cool and NVT
+ * production): thermostat 0 none, 1 rescale every rescale_every steps to temperature[r], 2 Bussi with coupling
+ * time bussi_tau at temperature[r], each replica's generator started afresh from seeds[r] (a new
+ * BussiThermostat, src/Thermostat.cpp:36-44). temperature may be NULL to keep the targets (thermostat 0 needs
+ * none). Steps of the next run are numbered from 1 again. */
+md_status md_batch_set_thermostat(md_batch* b, int thermostat, int rescale_every, double bussi_tau,
+                                  const double* temperature, const uint64_t* seeds);
 /* Potential energy, virial, inside-cutoff pair count and kinetic energy of each replica's current state
  * (replicas entries each; any may be NULL). */
 md_status md_batch_energy(md_batch* b, double* pe, double* virial, double* ke, double* inside);

@@ -8,15 +8,19 @@
 #include "md_common.cuh"
 #include "md_fp32.cuh"
 #include "md_fp64.cuh"
+#include "md_fx32.cuh"
 #include "md_fx64.cuh"
+#include "md_graph.cuh"
 #include "md_nlist.cuh"
 #include "md_scan.cuh"
 #include "md_tiles.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <random>
 #include <string>
@@ -28,6 +32,13 @@ namespace {
 
 thread_local std::string g_error;
 thread_local uint64_t* g_launches = nullptr;  // launch counter of the system the current call works on
+// While md_run captures a chunk graph: the graph's profiling events (force kernels are bracketed by external
+// event records) and the flag a tile force kernel sets when its tile outgrows the recorded shared memory
+thread_local std::vector<cudaEvent_t>* g_capture_prof = nullptr;
+thread_local size_t g_capture_prof_next = 0;  // next unused event of *g_capture_prof (created before capture)
+thread_local int* g_graph_overflow = nullptr;
+thread_local bool g_capturing = false;  // function attributes are set before a capture, not inside it
+std::atomic<uint64_t> g_serial{1};  // serial numbers of force fields and lists (md_run's graphs record them)
 
 md_status fail(md_status s, const std::string& msg) {
     g_error = msg;
@@ -94,6 +105,13 @@ constexpr int kThreads = 256;
 // kernels) counts against the same 48 KB default, so the threshold leaves room for it.
 constexpr size_t kSmemNoOptIn = 32 * 1024;
 
+// Opt a kernel in to `bytes` of dynamic shared memory (not while md_run captures a graph: it sets them first)
+template <typename K>
+cudaError_t allow_smem(K kernel, size_t bytes) {
+    if (g_capturing || bytes <= kSmemNoOptIn) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+
 // Slots of md_system::scal (device scalars)
 constexpr int kScalFactor = 1;  // [1] velocity scale factor, [2] 1 to apply it / 0 to skip
 constexpr int kScalKE = 4;      // [4] kinetic energy ([5] scratch of the blocked sum)
@@ -102,6 +120,15 @@ constexpr int kScalR1 = 6;      // [6] r1, [7] chi2 of one Bussi step
 }  // namespace
 
 // ---- handles ---------------------------------------------------------------------------------------------
+
+// One chunk graph of md_run (md_run_graph.inl)
+struct RunGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaEvent_t> prof;  // (before, after) each force kernel, when recorded with profiling on
+    int rdf_samples = 0;            // g(r) samples per launch
+    uint64_t kernels = 0;           // kernels per launch outside the rebuild bodies
+    uint64_t body_kernels = 0;      // kernels of one rebuild body
+};
 
 struct md_system {
     int device = 0;
@@ -128,7 +155,31 @@ struct md_system {
     cudaEvent_t frame_ready = nullptr;
     // resident grid of k_force_fp32_resident<fixed, energy> (blocks that fit on the SMs at once), 0 until known
     unsigned fp32_resident[2][2] = {{0, 0}, {0, 0}};
+    unsigned fx32_resident[2] = {0, 0};  // likewise for k_force_fx32<energy>
+    // md_run's chunk graphs (md_run_graph.inl): the cache, chunk length (0: host loop), test flags, the stream
+    // the rebuild bodies are captured on, device counters ([0] rebuilds, [1] overflow), per-chunk records and
+    // Bussi draws, the snapshot a chunk restarts from, and the canonical buffer of each double-buffered array
+    std::map<std::string, RunGraph> graphs;
+    int graph_chunk = 64;
+    int graph_flags = 0;
+    cudaStream_t body_stream = nullptr;
+    DevBuf<int> graph_state, snap_flag;
+    DevBuf<double> chunk_rec, chunk_noise;
+    DevBuf<double4> snap_pos, snap_ref, pos_save;
+    DevBuf<double> snap_vel, snap_force, snap_mass;
+    DevBuf<uint64_t> snap_ids;
+    DevBuf<unsigned long long> snap_hist;
+    void* canon[7] = {};
+    uint64_t graph_launches = 0, graph_recoveries = 0;
 };
+
+void drop_run_graphs(md_system* s) {
+    for (auto& g : s->graphs) {
+        if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
+        for (cudaEvent_t e : g.second.prof) cudaEventDestroy(e);
+    }
+    s->graphs.clear();
+}
 
 // After k_permute: the permuted arrays become the system's, the old ones its reorder buffers. No device
 // pointer of a system outlives a call, so the swap is invisible outside the library.
@@ -155,6 +206,7 @@ struct md_cells {
 };
 
 struct md_nlist {
+    uint64_t serial = g_serial++;
     double rc = 0, skin = 0, rl = 0, rl2 = 0, max_disp2 = 0;
     bool reverse = false;
     int device = -1;
@@ -177,8 +229,15 @@ struct md_nlist {
     TileGeom tiles_geom{};
     int build_kernel = -1;  // list build of the last rebuild: 0 thread per particle, 1 tiles
     int build_pin = -1;     // set by md_nlist_set_build_variant (-1: tiles where available)
-    int variant[4] = {-1, -1, -1, -1};  // force kernel per precision (0 global gathers, 1 tile; -1 untuned)
-    int pinned[4] = {-1, -1, -1, -1};   // set by md_nlist_set_force_variant
+    int variant[5] = {-1, -1, -1, -1, -1};  // force kernel per precision (0 global gathers, 1 tile; -1 untuned)
+    int pinned[5] = {-1, -1, -1, -1, -1};   // set by md_nlist_set_force_variant
+    uint64_t builds = 0;                    // list builds so far (names the rows of the last one)
+    // MD_PREC_FX32's near-first copy of the rows (k_rows_near_first) and its (near groups, groups) counts, for
+    // build nf_build with the near radius^2 nf_near2
+    DevBuf<uint32_t> rows_nf;
+    DevBuf<int2> counts_nf;
+    uint64_t nf_build = 0;
+    double nf_near2 = -1.0;
     int rebuilds = 0;
     uint64_t pairs = 0;
     bool pairs_ready = false;  // half_off and pairs match the last build
@@ -186,6 +245,7 @@ struct md_nlist {
 };
 
 struct md_forcefield {
+    uint64_t serial = g_serial++;
     double eps = 1, sigma = 1, rc = 2.5;
     LJ lj{};
     int precision = MD_PREC_FP64;
@@ -411,9 +471,7 @@ md_status nlist_build(md_nlist* nl, md_system* s) {
             BuildParams bp{nl->rl2, static_cast<float>(nl->rl2 - margin), static_cast<float>(nl->rl2 + margin),
                            nl->cap, static_cast<uint32_t>(n)};
             const size_t smem = sizeof(float4) * tg.max_staged;
-            if (smem > kSmemNoOptIn)
-                MD_CUDA(cudaFuncSetAttribute(k_nlist_build_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem)));
+            MD_CUDA(allow_smem(k_nlist_build_tile, smem));
             k_nlist_build_tile<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
                 nl->frames.p, s->pos.p, nl->grid.start.p, nl->cell_sorted.p, tg, bp, cell_offsets(nl, s), nl->rows.p,
                 nl->counts.p, nl->flags.p + 1);
@@ -435,6 +493,7 @@ md_status nlist_build(md_nlist* nl, md_system* s) {
         if (attempt == 3) return fail(MD_ERR_CAPACITY, "neighbour row capacity could not be met");
     }
     nl->pairs_ready = false;  // the half-list offsets and pair count are computed when first needed
+    nl->builds++;
     nl->n = s->n;
     nl->sys = s;
     nl->layout = s->layout;
@@ -482,6 +541,11 @@ md_status check_cutoff(const md_forcefield* ff, const md_system* s) {
 // md_profile_*: a CUDA event on the system's stream before and after each list force kernel
 md_status profile_mark(md_system* s) {
     if (!s->profile) return MD_OK;
+    if (g_capture_prof) {  // inside a graph capture: an event record node, recorded at every launch
+        if (g_capture_prof_next >= g_capture_prof->size()) return fail(MD_ERR_STATE, "graph profile events exhausted");
+        MD_CUDA(cudaEventRecordWithFlags((*g_capture_prof)[g_capture_prof_next++], s->stream, cudaEventRecordExternal));
+        return MD_OK;
+    }
     if (s->events_used == s->events.size()) {
         cudaEvent_t e;
         MD_CUDA(cudaEventCreate(&e));
@@ -612,9 +676,7 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
                 if (variant == 1) {
                     const TileGeom& tg = nl->tiles_geom;
                     const size_t smem = sizeof(double4) * tg.max_staged;
-                    if (smem > kSmemNoOptIn)
-                        MD_CUDA(cudaFuncSetAttribute(k_force_fp64_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     static_cast<int>(smem)));
+                    MD_CUDA(allow_smem(k_force_fp64_tile, smem));
                     const KickArgs ka{kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
                     k_force_fp64_tile<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
                         s->pos.p, n, nl->grid.start.p, nl->cell_sorted.p, tg, ff->lj, nl->rows.p, nl->cap,
@@ -730,6 +792,7 @@ md_status kick_async(md_system* s, double dt) {
 }  // namespace
 
 #include "md_abi_float.inl"
+#include "md_run_graph.inl"
 
 // ---- library ---------------------------------------------------------------------------------------------
 
@@ -798,6 +861,8 @@ md_status md_system_destroy(md_system* s) {
     for (cudaEvent_t e : s->events) cudaEventDestroy(e);
     if (s->frame_ready) cudaEventDestroy(s->frame_ready);
     if (s->host_scal) cudaFreeHost(s->host_scal);
+    drop_run_graphs(s);
+    if (s->body_stream) cudaStreamDestroy(s->body_stream);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -1185,8 +1250,8 @@ md_status md_nlist_info(const md_nlist* nl, uint64_t* pair_count, int* rebuild_c
 }
 
 md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant) {
-    if (!nl || precision < MD_PREC_FP64 || precision > MD_PREC_FX64 || variant < -1 || variant > 4 ||
-        (precision == MD_PREC_FX64 && variant >= 1) || (precision == MD_PREC_FP64 && variant >= 3))
+    if (!nl || precision < MD_PREC_FP64 || precision > MD_PREC_FX32 || variant < -1 || variant > 4 ||
+        (precision >= MD_PREC_FX64 && variant >= 1) || (precision == MD_PREC_FP64 && variant >= 3))
         return fail(MD_ERR_INVALID, "md_nlist_set_force_variant: bad arguments");
     nl->pinned[precision] = variant;
     nl->variant[precision] = -1;
@@ -1194,7 +1259,7 @@ md_status md_nlist_set_force_variant(md_nlist* nl, int precision, int variant) {
 }
 
 md_status md_nlist_force_variant(const md_nlist* nl, int precision, int* variant) {
-    if (!nl || !variant || precision < MD_PREC_FP64 || precision > MD_PREC_FX64)
+    if (!nl || !variant || precision < MD_PREC_FP64 || precision > MD_PREC_FX32)
         return fail(MD_ERR_INVALID, "md_nlist_force_variant: bad arguments");
     *variant = nl->variant[precision];
     return MD_OK;
@@ -1305,7 +1370,7 @@ md_status md_forcefield_shift(const md_forcefield* ff, double* shift) {
 }
 
 md_status md_forcefield_set_precision(md_forcefield* ff, int precision) {
-    if (!ff || precision < MD_PREC_FP64 || precision > MD_PREC_FX64) return fail(MD_ERR_INVALID, "bad precision");
+    if (!ff || precision < MD_PREC_FP64 || precision > MD_PREC_FX32) return fail(MD_ERR_INVALID, "bad precision");
     ff->precision = precision;
     return MD_OK;
 }
@@ -1467,6 +1532,42 @@ md_status md_run(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64
     if (o.rdf && o.rdf_every <= 0) return fail(MD_ERR_INVALID, "rdf_every must be positive");
     ff->device = s->device;
     return run_steps(s, ff, nl, dt, n_steps, o, pe, ke, virial);
+}
+
+md_status md_run_prepare(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
+                         const md_run_options* opts, int record) {
+    if (!s || !ff || !nl || n_steps < 0) return fail(MD_ERR_INVALID, "md_run_prepare: bad arguments");
+    MD_TRY(use_system(s));
+    MD_TRY(check_cutoff(ff, s));
+    md_run_options o{};
+    if (opts) o = *opts;
+    if (o.thermostat == 1 && o.rescale_every <= 0) return fail(MD_ERR_INVALID, "rescale_every must be positive");
+    if (o.rdf && o.rdf_every <= 0) return fail(MD_ERR_INVALID, "rdf_every must be positive");
+    ff->device = s->device;
+    if (!graph_mode_ok(s, ff, nl, n_steps)) return MD_OK;  // md_run would take the host path: nothing to prepare
+    MD_TRY(graph_prepare(s, ff, nl, dt, n_steps, o, (record & 1) != 0, (record & 2) != 0));
+    return sync(s);
+}
+
+md_status md_system_set_graph(md_system* s, int chunk_steps, int flags) {
+    if (!s || chunk_steps < 0 || chunk_steps > 1024 || (flags & ~MD_GRAPH_EXACT_TILES))
+        return fail(MD_ERR_INVALID, "md_system_set_graph: bad arguments");
+    MD_TRY(use_system(s));
+    MD_TRY(sync(s));
+    drop_run_graphs(s);
+    s->graph_chunk = chunk_steps;
+    s->graph_flags = flags;
+    return MD_OK;
+}
+
+md_status md_system_graph_info(const md_system* s, int* chunk_steps, uint64_t* graphs, uint64_t* launches,
+                               uint64_t* recoveries) {
+    if (!s) return fail(MD_ERR_INVALID, "null system");
+    if (chunk_steps) *chunk_steps = s->graph_chunk;
+    if (graphs) *graphs = s->graphs.size();
+    if (launches) *launches = s->graph_launches;
+    if (recoveries) *recoveries = s->graph_recoveries;
+    return MD_OK;
 }
 
 }  // extern "C"

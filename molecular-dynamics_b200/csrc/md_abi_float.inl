@@ -3,6 +3,11 @@
 
 namespace {
 
+// md_run's graph mode (md_run_graph.inl)
+bool graph_mode_ok(const md_system* s, const md_forcefield* ff, const md_nlist* nl, int64_t n_steps);
+md_status run_steps_graph(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
+                          const md_run_options& o, double* pe, double* ke, double* virial);
+
 FloatLJ float_lj(const md_forcefield* ff) {
     FloatLJ f{};
     f.sig2 = static_cast<float>(ff->lj.sig2);
@@ -138,11 +143,112 @@ md_status forces_list_fx64_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
     return MD_OK;
 }
 
+// MD_PREC_FX32 evaluates pairs closer than this many sigma (plus the skin, at the list build) in double
+constexpr double kFx32NearSigma = 1.3;
+
+// MD_PREC_FX32's near-first rows of the list's last build (k_rows_near_first), made once per build and near radius
+md_status ensure_near_first(md_forcefield* ff, md_system* s, md_nlist* nl) {
+    const int n = static_cast<int>(s->n);
+    const double near = kFx32NearSigma * ff->sigma + nl->skin;
+    const double near2 = near * near;
+    if (n == 0 || (nl->nf_build == nl->builds && nl->nf_near2 == near2)) return MD_OK;
+    MD_CUDA(nl->rows_nf.reserve(row_buffer_entries(n, nl->cap)));
+    MD_CUDA(nl->counts_nf.reserve(n));
+    k_rows_near_first<<<blocks_for(n, 128), 128, 0, s->stream>>>(nl->ref_pos.p, n, s->box, near2, nl->rows.p, nl->cap,
+                                                                 nl->counts.p, nl->rows_nf.p, nl->counts_nf.p);
+    MD_CHECK_LAUNCH();
+    nl->nf_build = nl->builds;
+    nl->nf_near2 = near2;
+    return MD_OK;
+}
+
+// MD_PREC_FX32 list forces: after each list build the rows are reordered near-first (k_rows_near_first, once per
+// build and near radius); then the fixed-point frames and k_force_fx32 on a resident grid, with the closing kick,
+// kinetic energy and optionally the next drift fused as in forces_list_fx64_async. Boxes under 3 cells per side
+// take the MD_PREC_FX64 small-box kernel (every pair in double).
+md_status forces_list_fx32_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt,
+                                 bool* fused_ke, bool fixed_fresh, bool fuse_drift) {
+    if (!nl->use_cells) return forces_list_fx64_async(ff, s, nl, want_energy, kick_dt, fused_ke, fixed_fresh, fuse_drift);
+    const int n = static_cast<int>(s->n);
+    const bool kick = kick_dt > 0.0;
+    const Fx64LJ dlj = fx64_lj(ff);
+    FloatLJ flj = float_lj(ff);
+    // the float r^2 of an exact separation rounded once per component is within ~6e-7 of r^2 (relative): a
+    // shell of 1e-5 r_c^2 holds every pair whose float and exact cutoff tests could disagree
+    flj.band = static_cast<float>(1e-5 * ff->lj.rc2);
+    MD_CUDA(ff->fx_acc.reserve(4));
+    if (want_energy || kick) MD_CUDA(cudaMemsetAsync(ff->fx_acc.p, 0, 4 * sizeof(long long), s->stream));
+    auto* acc = reinterpret_cast<unsigned long long*>(ff->fx_acc.p);
+    nl->variant[MD_PREC_FX32] = 0;
+    if (n > 0) {
+        MD_TRY(ensure_near_first(ff, s, nl));
+        MD_CUDA(nl->iframes.reserve(n));
+        if (!fixed_fresh) {
+            k_frames_fixed<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(s->pos.p, n, nl->cell_sorted.p,
+                                                                               nl->grid.ncps, cell_side(nl, s), s->box,
+                                                                               nl->iframes.p);
+            MD_CHECK_LAUNCH();
+        }
+        KickArgs ka{kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
+        const bool fuse = fuse_drift && kick;
+        if (fuse) {  // the next step's kick and drift, new positions and fixed-point frames to spare buffers
+            MD_CUDA(s->pos2.reserve(n));
+            MD_CUDA(nl->iframes2.reserve(n));
+            MD_CUDA(cudaMemsetAsync(nl->flags.p, 0, sizeof(int), s->stream));
+            ka.pos_in = s->pos.p;
+            ka.pos_out = s->pos2.p;
+            ka.iframes_out = nl->iframes2.p;
+            ka.ref_pos = nl->ref_pos.p;
+            ka.max_disp2 = nl->max_disp2;
+            ka.stale = nl->flags.p;
+            ka.cell_sorted = nl->cell_sorted.p;
+            ka.ncps = nl->grid.ncps;
+            ka.cell = cell_side(nl, s);
+            ka.dt = kick_dt;
+            ka.box = s->box;
+        }
+        const FixedOffsets offs = fixed_offsets(nl, s);
+        auto go = [&](auto kernel, unsigned& grid) -> md_status {
+            if (grid == 0) {
+                int sms = 0, per_sm = 0;
+                MD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+                MD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0));
+                grid = static_cast<unsigned>(std::max(1, sms * per_sm));
+            }
+            MD_TRY(profile_mark(s));
+            kernel<<<std::min(blocks_for(n, 128), grid), 128, 0, s->stream>>>(
+                nl->iframes.p, s->pos.p, n, s->box, dlj, flj, offs, nl->rows_nf.p, nl->cap, nl->counts_nf.p,
+                s->force.p, acc, ka);
+            MD_CHECK_LAUNCH();
+            return profile_mark(s);
+        };
+        if (want_energy)
+            MD_TRY(go(k_force_fx32<true>, s->fx32_resident[1]));
+        else
+            MD_TRY(go(k_force_fx32<false>, s->fx32_resident[0]));
+        if (fuse) {
+            swap_buffers(s->pos, s->pos2);
+            swap_buffers(nl->iframes, nl->iframes2);
+        }
+    }
+    const bool ke_fused = kick && n > 0;
+    if (want_energy || ke_fused) {
+        k_finish_float_energy<<<1, 1, 0, s->stream>>>(acc, ff->out.p, ff->inside_count.p,
+                                                      ke_fused ? s->scal.p + kScalKE : nullptr, 1.0 / kKineticScale,
+                                                      kEnergyUnit64);
+        MD_CHECK_LAUNCH();
+    }
+    if (fused_ke) *fused_ke = ke_fused;
+    return MD_OK;
+}
+
 // See forces_list_async. Every float kernel fuses the closing kick with a fixed-point kinetic energy.
 md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt,
                                   bool frames_fresh, bool* fused_ke, bool fuse_drift, bool fixed_fresh) {
     if (ff->precision == MD_PREC_FX64)
         return forces_list_fx64_async(ff, s, nl, want_energy, kick_dt, fused_ke, fixed_fresh, fuse_drift);
+    if (ff->precision == MD_PREC_FX32)
+        return forces_list_fx32_async(ff, s, nl, want_energy, kick_dt, fused_ke, fixed_fresh, fuse_drift);
     const int n = static_cast<int>(s->n);
     const bool fixed = ff->precision == MD_PREC_FP32FX;
     const bool kick = kick_dt > 0.0;
@@ -163,9 +269,10 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
             KickArgs drift{nullptr, nullptr, 0.0};
             auto launch = [&](int variant, bool with_kick, bool energy, double* tune_vel = nullptr,
                               const KickArgs* fused = nullptr) -> md_status {
-                const KickArgs ka = fused ? *fused
-                                          : tune_vel ? KickArgs{tune_vel, s->mass.p, 0.0}
-                                                     : KickArgs{with_kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
+                KickArgs ka = fused ? *fused
+                                    : tune_vel ? KickArgs{tune_vel, s->mass.p, 0.0}
+                                               : KickArgs{with_kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
+                ka.overflow = g_graph_overflow;
                 auto go = [&](auto rows_kernel, auto tile_kernel, auto prefetch_kernel, auto capped_kernel,
                               auto resident_kernel) -> md_status {
                     if (variant == 4) {
@@ -180,9 +287,7 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
                             nl->frames.p, s->pos.p, n, s->box, lj, offs, nl->rows.p, nl->cap, nl->counts.p, s->force.p,
                             acc, ka);
                     } else if (variant == 1) {
-                        if (smem > kSmemNoOptIn)
-                            MD_CUDA(cudaFuncSetAttribute(tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                         static_cast<int>(smem)));
+                        MD_CUDA(allow_smem(tile_kernel, smem));
                         tile_kernel<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
                             nl->frames.p, s->pos.p, n, nl->grid.start.p, nl->cell_sorted.p, tg, lj, offs, nl->rows.p,
                             nl->cap, nl->counts.p, s->force.p, acc, ka);
@@ -291,6 +396,20 @@ md_status kinetic_fixed_async(md_system* s, md_forcefield* ff) {
     return MD_OK;
 }
 
+// The histogram kernel of RadialDistribution::sample (src/RadialDistribution.cpp:11-30) on the system's stream; the
+// histogram must exist
+md_status rdf_kernel_async(md_rdf* r, md_system* s, md_nlist* nl) {
+    const int n = static_cast<int>(s->n);
+    if (n > 0) {
+        const size_t smem = sizeof(unsigned int) * r->bins;
+        MD_CUDA(allow_smem(k_rdf_sample, smem));
+        k_rdf_sample<<<blocks_for(n, kThreads), kThreads, smem, s->stream>>>(
+            s->pos.p, n, s->box, nl->rows.p, nl->cap, nl->counts.p, r->rmax * r->rmax, r->bin_width, r->bins, r->hist.p);
+        MD_CHECK_LAUNCH();
+    }
+    return MD_OK;
+}
+
 // RadialDistribution::sample (src/RadialDistribution.cpp:11-30) queued on the system's stream
 md_status rdf_sample_async(md_rdf* r, md_system* s, md_nlist* nl) {
     if (r->device < 0) {
@@ -298,20 +417,23 @@ md_status rdf_sample_async(md_rdf* r, md_system* s, md_nlist* nl) {
         MD_CUDA(r->hist.reserve(r->bins));
         MD_CUDA(cudaMemsetAsync(r->hist.p, 0, sizeof(unsigned long long) * r->bins, s->stream));
     }
-    const int n = static_cast<int>(s->n);
-    if (n > 0) {
-        const size_t smem = sizeof(unsigned int) * r->bins;
-        if (smem > kSmemNoOptIn)
-            MD_CUDA(cudaFuncSetAttribute(k_rdf_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-        k_rdf_sample<<<blocks_for(n, kThreads), kThreads, smem, s->stream>>>(
-            s->pos.p, n, s->box, nl->rows.p, nl->cap, nl->counts.p, r->rmax * r->rmax, r->bin_width, r->bins, r->hist.p);
-        MD_CHECK_LAUNCH();
-    }
+    MD_TRY(rdf_kernel_async(r, s, nl));
     // src/RadialDistribution.cpp:18-22
     const double volume = std::pow(s->box.L, 3);
     r->particles = static_cast<double>(s->n);
     r->density = r->particles / volume;
     r->samples++;
+    return MD_OK;
+}
+
+// The force-kernel times of one chunk graph's launch (md_profile_*): the stream must have been synchronised
+md_status collect_graph_profile(md_system* s, const RunGraph& g) {
+    for (size_t k = 0; k + 1 < g.prof.size(); k += 2) {
+        float ms = 0.f;
+        MD_CUDA(cudaEventElapsedTime(&ms, g.prof[k], g.prof[k + 1]));
+        s->profile_ms += ms;
+        s->profile_count++;
+    }
     return MD_OK;
 }
 
@@ -321,6 +443,7 @@ md_status rdf_sample_async(md_rdf* r, md_system* s, md_nlist* nl) {
 // kernel fuses with the closing kick, and recompute it after a thermostat.
 md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
                     const md_run_options& o, double* pe, double* ke, double* virial) {
+    if (graph_mode_ok(s, ff, nl, n_steps)) return run_steps_graph(s, ff, nl, dt, n_steps, o, pe, ke, virial);
     const double bussi_c = o.thermostat == 2 ? std::exp(-dt / o.bussi_tau) : 0.0;  // src/Thermostat.cpp:46
     DevBuf<double> noise;
     if (o.thermostat == 2 && n_steps > 0) {
@@ -334,7 +457,7 @@ md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, in
     const bool want_energy = pe || virial;
     const bool exact_ke = ff->precision == MD_PREC_FP64;
     const bool float_mode = ff->precision == MD_PREC_FP32FX || ff->precision == MD_PREC_FP32 ||
-                            ff->precision == MD_PREC_FX64;
+                            ff->precision == MD_PREC_FX64 || ff->precision == MD_PREC_FX32;
     bool drifted = false;  // the previous step's force kernel already made this step's kick and drift
     for (int64_t k = 0; k < n_steps; ++k) {
         const int64_t step = o.first_step + k;

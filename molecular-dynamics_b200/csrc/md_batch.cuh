@@ -652,6 +652,12 @@ __global__ void k_b_finish_fp64(int R, unsigned long long* __restrict__ acc, uns
     s[0] = s[1] = s[2] = s[3] = 0;
 }
 
+// The inside-cutoff count of every replica's last force evaluation into a record row (doubles)
+__global__ void k_b_record_inside(int R, const unsigned long long* __restrict__ inside, double* __restrict__ out) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < R) out[r] = static_cast<double>(inside[r]);
+}
+
 // ---- kinetic energy and thermostats ---------------------------------------------------------------------------
 
 // System::kineticEnergy's blocked sum (k_kinetic_blocks) per replica: one warp per 1024-particle block of a

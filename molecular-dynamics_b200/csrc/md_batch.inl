@@ -77,6 +77,42 @@ struct md_batch {
 namespace {
 
 constexpr int kMaxAttempts = 4;
+constexpr int kRecRows = 4;  // per recorded step: potential energy, virial, kinetic energy, inside-cutoff pairs
+
+// Steps per chunk graph: chunk_steps (100 by default) rounded up to a multiple of the sampling and thermostat
+// periods, so every chunk starts on a multiple of both
+int b_chunk_len(const md_batch_options& o, int thermo_every) {
+    auto gcd = [](int64_t x, int64_t y) {
+        while (y) {
+            const int64_t t = x % y;
+            x = y;
+            y = t;
+        }
+        return x;
+    };
+    int64_t period = 1;
+    for (int64_t p : {static_cast<int64_t>(o.energy_every), static_cast<int64_t>(thermo_every)})
+        if (p > 0) period = period / gcd(period, p) * p;
+    int64_t want = o.chunk_steps > 0 ? o.chunk_steps : 100;
+    want = (want + period - 1) / period * period;
+    return static_cast<int>(std::min<int64_t>(want, 1 << 20));
+}
+
+// The buffers sized by the chunk length: Bussi draws (device, and two chunks' worth pinned on the host) and the
+// records of one chunk (device and pinned host)
+md_status b_chunk_buffers(md_batch* b) {
+    const size_t R = static_cast<size_t>(b->R), C = static_cast<size_t>(b->chunk);
+    const int every = b->opt.energy_every;
+    const size_t samples = every > 0 ? C / every : 0;
+    MD_CUDA(b->noise.reserve(2 * C * R));
+    MD_CUDA(b->rec.reserve(std::max<size_t>(1, kRecRows * samples * R)));
+    if (b->h_noise) cudaFreeHost(b->h_noise);
+    if (b->h_rec) cudaFreeHost(b->h_rec);
+    b->h_noise = b->h_rec = nullptr;
+    MD_CUDA(cudaMallocHost(reinterpret_cast<void**>(&b->h_noise), sizeof(double) * 4 * C * R));
+    MD_CUDA(cudaMallocHost(reinterpret_cast<void**>(&b->h_rec), sizeof(double) * std::max<size_t>(1, kRecRows * samples * R)));
+    return MD_OK;
+}
 
 md_status use_batch(md_batch* b) {
     g_launches = &b->launches;
@@ -259,6 +295,10 @@ md_status b_enqueue_step(md_batch* b, int k, int64_t step, double* rec) {
         if (thermo) MD_TRY(b_kinetic_fp64(b, false, b->ke.p));
         if (sample) MD_TRY(b_energy_fp64(b, rec, rec + R));
     }
+    if (sample) {
+        k_b_record_inside<<<per_replica(b, kThreads), kThreads, 0, st>>>(R, b->inside.p, rec + 3 * R);
+        MD_CHECK_LAUNCH();
+    }
     if (thermo) {
         const double* r1 = b->noise.p + static_cast<size_t>(k) * R;
         const double* chi2 = b->noise.p + static_cast<size_t>(b->chunk + k) * R;
@@ -281,7 +321,7 @@ md_status b_enqueue_step(md_batch* b, int k, int64_t step, double* rec) {
     return MD_OK;
 }
 
-// The graph of `len` steps (recorded energies at every energy_every-th step into rec[(s * 3 + q) * R + r])
+// The graph of `len` steps (recorded energies at every energy_every-th step into rec[(s * kRecRows + q) * R + r])
 md_status b_graph(md_batch* b, int len, cudaGraphExec_t* out, uint64_t* kernels) {
     auto it = b->graphs.find(len);
     if (it != b->graphs.end()) {
@@ -298,7 +338,7 @@ md_status b_graph(md_batch* b, int len, cudaGraphExec_t* out, uint64_t* kernels)
     const int every = b->opt.energy_every;
     for (int k = 0; k < len && st == MD_OK; ++k) {
         const int64_t step = k + 1;  // chunks start at multiples of the thermostat and sampling periods
-        double* rec = every > 0 && step % every == 0 ? b->rec.p + static_cast<size_t>(step / every - 1) * 3 * b->R
+        double* rec = every > 0 && step % every == 0 ? b->rec.p + static_cast<size_t>(step / every - 1) * kRecRows * b->R
                                                      : nullptr;
         st = b_enqueue_step(b, k, step, rec);
     }
@@ -526,23 +566,7 @@ md_status md_batch_create(int device, int replicas, const int64_t* n_atoms, cons
     b->max_disp2 = 0.25 * o.skin * o.skin;  // src/NeighbourList.cpp:7
     b->bussi_c = o.thermostat == 2 ? std::exp(-o.dt / o.bussi_tau) : 0.0;  // src/Thermostat.cpp:46
     b->thermo_every = o.thermostat == 2 ? 1 : (o.thermostat == 1 ? o.rescale_every : 0);
-    {
-        // chunks start on multiples of the sampling and thermostat periods
-        auto gcd = [](int64_t x, int64_t y) {
-            while (y) {
-                const int64_t t = x % y;
-                x = y;
-                y = t;
-            }
-            return x;
-        };
-        int64_t period = 1;
-        for (int64_t p : {static_cast<int64_t>(o.energy_every), static_cast<int64_t>(b->thermo_every)})
-            if (p > 0) period = period / gcd(period, p) * p;
-        int64_t want = o.chunk_steps > 0 ? o.chunk_steps : 100;
-        want = (want + period - 1) / period * period;
-        b->chunk = static_cast<int>(std::min<int64_t>(want, 1 << 20));
-    }
+    b->chunk = b_chunk_len(o, b->thermo_every);
     // layout
     b->reps_h.resize(replicas);
     std::vector<int> tile_rep(b->tiles), chunk_rep;
@@ -614,13 +638,9 @@ md_status md_batch_create(int device, int replicas, const int64_t* n_atoms, cons
     for (auto* buf : {&b->rebuilds, &b->inside, &b->s_rebuilds}) chk(buf->reserve(R));
     for (auto* buf : {&b->ke, &b->tmp_pe, &b->tmp_w}) chk(buf->reserve(R));
     chk(b->chunk_sums.reserve(b->chunks));
-    chk(b->noise.reserve(2 * static_cast<size_t>(b->chunk) * R));
-    const int samples = o.energy_every > 0 ? b->chunk / o.energy_every : 0;
-    chk(b->rec.reserve(std::max<size_t>(1, 3 * static_cast<size_t>(samples) * R)));
+    if (st == MD_OK) st = b_chunk_buffers(b);
     chk(b->scale.reserve(R));
     chk(b->s_scale.reserve(R));
-    chk(cudaMallocHost(reinterpret_cast<void**>(&b->h_noise), sizeof(double) * 4 * static_cast<size_t>(b->chunk) * R));
-    chk(cudaMallocHost(reinterpret_cast<void**>(&b->h_rec), sizeof(double) * std::max<size_t>(1, 3 * samples * R)));
     chk(cudaMallocHost(reinterpret_cast<void**>(&b->h_flags), sizeof(int) * 4));
     if (st == MD_OK) {
         chk(cudaMemcpyAsync(b->reps.p, b->reps_h.data(), sizeof(BRep) * R, cudaMemcpyHostToDevice, b->stream));
@@ -739,7 +759,40 @@ md_status md_batch_force_variant(const md_batch* b, int* variant, int* count, in
     return MD_OK;
 }
 
+md_status md_batch_set_thermostat(md_batch* b, int thermostat, int rescale_every, double bussi_tau,
+                                  const double* temperature, const uint64_t* seeds) {
+    if (!b || thermostat < 0 || thermostat > 2 || (thermostat == 1 && rescale_every <= 0) ||
+        (thermostat == 2 && (!(bussi_tau > 0.0) || !seeds)) || (thermostat != 0 && !temperature))
+        return fail(MD_ERR_INVALID, "md_batch_set_thermostat: bad arguments");
+    MD_TRY(use_batch(b));
+    MD_TRY(bsync(b));
+    b->opt.thermostat = thermostat;
+    if (thermostat == 1) b->opt.rescale_every = rescale_every;
+    if (thermostat == 2) b->opt.bussi_tau = bussi_tau;
+    b->bussi_c = thermostat == 2 ? std::exp(-b->opt.dt / bussi_tau) : 0.0;  // src/Thermostat.cpp:46
+    b->thermo_every = thermostat == 2 ? 1 : (thermostat == 1 ? rescale_every : 0);
+    if (temperature) {
+        for (int r = 0; r < b->R; ++r) b->reps_h[r].temperature = temperature[r];
+        MD_CUDA(cudaMemcpyAsync(b->reps.p, b->reps_h.data(), sizeof(BRep) * b->R, cudaMemcpyHostToDevice, b->stream));
+    }
+    if (thermostat == 2) {  // a new BussiThermostat per replica (src/Thermostat.cpp:36-44): a fresh generator
+        b->rng.clear();
+        for (int r = 0; r < b->R; ++r) b->rng.emplace_back(seeds[r]);
+    }
+    const int chunk = b_chunk_len(b->opt, b->thermo_every);
+    if (chunk != b->chunk) {
+        b->chunk = chunk;
+        MD_TRY(b_chunk_buffers(b));
+    }
+    b_drop_graphs(b);
+    return bsync(b);
+}
+
 md_status md_batch_run(md_batch* b, int64_t n_steps, double* pe, double* virial, double* ke) {
+    return md_batch_run_records(b, n_steps, pe, virial, ke, nullptr);
+}
+
+md_status md_batch_run_records(md_batch* b, int64_t n_steps, double* pe, double* virial, double* ke, double* inside) {
     if (!b || n_steps < 0) return fail(MD_ERR_INVALID, "md_batch_run: bad arguments");
     MD_TRY(use_batch(b));
     const int R = b->R, every = b->opt.energy_every;
@@ -763,7 +816,7 @@ md_status md_batch_run(md_batch* b, int64_t n_steps, double* pe, double* virial,
             b->launches += kernels;
             const int samples = every > 0 ? len / every : 0;
             if (samples > 0)
-                MD_CUDA(cudaMemcpyAsync(b->h_rec, b->rec.p, sizeof(double) * 3 * samples * R, cudaMemcpyDeviceToHost,
+                MD_CUDA(cudaMemcpyAsync(b->h_rec, b->rec.p, sizeof(double) * kRecRows * samples * R, cudaMemcpyDeviceToHost,
                                         b->stream));
             MD_CUDA(cudaMemcpyAsync(b->h_flags, b->flags.p, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
             // the next chunk's draws are made while this one runs
@@ -779,10 +832,11 @@ md_status md_batch_run(md_batch* b, int64_t n_steps, double* pe, double* virial,
             for (int s = 0; s < samples; ++s) {
                 const int64_t row = done / (every > 0 ? every : 1) + s;
                 for (int r = 0; r < R; ++r) {
-                    const double* h = b->h_rec + static_cast<size_t>(s) * 3 * R;
+                    const double* h = b->h_rec + static_cast<size_t>(s) * kRecRows * R;
                     if (pe) pe[row * R + r] = h[r];
                     if (virial) virial[row * R + r] = h[R + r];
                     if (ke) ke[row * R + r] = h[2 * R + r];
+                    if (inside) inside[row * R + r] = h[3 * R + r];
                 }
             }
         }

@@ -90,6 +90,7 @@ struct KickArgs {
     double cell = 0.0;
     double dt = 0.0;
     Box box{};
+    int* overflow = nullptr;  // set to 1 by a tile kernel whose staged tile outgrew its shared memory
 };
 
 // The truncated potential's force jumps by |F(r_c)| at the cutoff, so a pair whose float r^2 sits within
@@ -211,6 +212,19 @@ struct FloatAcc {
         if (kEnergy) {
             e_fx += __float2ll_rn(ge * kEnergyScale);
             w_fx += __float2ll_rn(gw * kEnergyScale);
+        }
+    }
+    // A float group whose energy and virial go into the finer 2^-30 units of the double groups (MD_PREC_FX32,
+    // whose rows hold both kinds); forces in the same 2^-32 units (the products with 2^32 and 2^30 are exact)
+    __device__ __forceinline__ void add_group_fine(float gx, float gy, float gz, float ge, float gw, long long& e_fx,
+                                                   long long& w_fx) {
+        static_assert(kFixed, "fine groups accumulate in fixed point");
+        ax += __float2ll_rn(gx * kForceScale);
+        ay += __float2ll_rn(gy * kForceScale);
+        az += __float2ll_rn(gz * kForceScale);
+        if (kEnergy) {
+            e_fx += __float2ll_rn(ge * static_cast<float>(kEnergyScale64));
+            w_fx += __float2ll_rn(gw * static_cast<float>(kEnergyScale64));
         }
     }
     // A group summed in double (MD_PREC_FX64): the same fixed-point units, rounded from double

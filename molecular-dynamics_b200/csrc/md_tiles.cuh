@@ -316,7 +316,10 @@ __global__ void __launch_bounds__(kTileThreads) k_nlist_build_tile(
                     const int gs = t.gstart[sc];
                     scan(s_q + t.off[sc], gs, 0, min(t.count[sc], i - gs), qo, code);
                 }
-        counts[i] = make_int2(own, cnt - own);
+        // a row past the capacity keeps counts within it (the entries written), so kernels that read the rows
+        // before the host sees max_count stay in bounds; max_count reports the full length
+        const int own_c = min(own, bp.cap), cnt_c = min(cnt, bp.cap);
+        counts[i] = make_int2(own_c, cnt_c - own_c);
         const int padded = (cnt + 7) & ~7;
         for (int s = cnt; s < padded && s < bp.cap; ++s) row[(s >> 2) * 128 + (s & 3)] = bp.sentinel | (kSentinelCode << kCodeShift);
         atomicMax(max_count, padded);
@@ -341,7 +344,10 @@ __global__ void __launch_bounds__(kTileThreads) k_force_fp32_tile(
     tile_tables(g, cell_start, t);
     const int span = t.kk + 2;
     const int sentinel_slot = g.max_staged;
-    if (t.total > g.max_staged) return;  // cannot happen after a build that checked the same bound
+    if (t.total > g.max_staged) {  // the bound recorded in a graph was outgrown: the host reruns the chunk
+        if (kick.overflow && threadIdx.x == 0) *kick.overflow = 1;
+        return;
+    }
     stage_tile(frames, s_q, t);
     if (threadIdx.x == 0) s_q[sentinel_slot] = make_float4(kSentinelCoord, kSentinelCoord, kSentinelCoord, 0.f);
     for (int e = threadIdx.x; e < t.kk * 32; e += blockDim.x) {

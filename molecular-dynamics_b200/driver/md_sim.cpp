@@ -1,7 +1,7 @@
 // md_sim for the GPU build: the reference's command-line driver (src/main.cpp of nhantran1711/molecular-dynamics)
 // rebuilt over the drop-in classes, with the same flags, stdout tables, CSV columns and machine-readable
 // RESULT line, so bench/benchmark.py and bench/validate.py can drive it unchanged. Two additions:
-//   --precision fp64|fp32fx|fp32|fx64   force precision (--mixed is fp32fx)
+//   --precision fp64|fp32fx|fp32|fx64|fx32   force precision (--mixed is fp32fx)
 //   --list-start                   initial forces from the neighbour list instead of the O(N^2) pass
 //   --device N                     CUDA device
 #include "Forcefield.hpp"
@@ -50,7 +50,7 @@ void usage() {
                  "Usage: md_sim [cellsPerSide] [--brute] [--dt X] [--skin X] [--cutoff X] [--equil N] [--steps N] "
                  "[--density X]\n              [--temperature X] [--nvt] [--seed N] [--melt] [--csv PATH] [--rdf PATH] "
                  "[--xyz PATH] [--xyz-every N]\n              [--deterministic] [--mixed] [--quiet] "
-                 "[--precision fp64|fp32fx|fp32|fx64] [--list-start] [--device N]\n");
+                 "[--precision fp64|fp32fx|fp32|fx64|fx32] [--list-start] [--device N]\n");
 }
 
 // Whole-string numeric parse with range checks (the reference's CommandLine.hpp contract)
@@ -103,7 +103,7 @@ bool parse(int argc, char** argv, Options& o) {
         else return false;
     }
     if (!o.precision.empty() && o.precision != "fp64" && o.precision != "fp32fx" && o.precision != "fp32" &&
-        o.precision != "fx64")
+        o.precision != "fx64" && o.precision != "fx32")
         return false;
     return o.cells > 0 && o.dt > 0.0 && o.skin > 0.0 && o.cutoff > 0.0 && o.density > 0.0 && o.temperature > 0.0 &&
            o.xyzEvery > 0 && o.steps > 0 && o.equil >= 0;
@@ -132,6 +132,7 @@ int run(const Options& o) {
     if (o.precision == "fp32fx") ff.setPrecision(LennardJonesForceField::Precision::FloatFixedPoint);
     if (o.precision == "fp32") ff.setPrecision(LennardJonesForceField::Precision::Float);
     if (o.precision == "fx64") ff.setPrecision(LennardJonesForceField::Precision::FixedDouble);
+    if (o.precision == "fx32") ff.setPrecision(LennardJonesForceField::Precision::FixedMixed);
     if (o.mixed && (o.deterministic || !o.list)) {
         std::fprintf(stderr, "--mixed applies to the default neighbour list path only\n");
         return 1;

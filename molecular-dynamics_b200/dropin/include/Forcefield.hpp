@@ -3,7 +3,8 @@
 // GPU (md_forcefield_*, md_forces_*). Every mode is deterministic on the device; setDeterministic(true) keeps
 // the reference's requirement of a list with a reverse index. setMixedPrecision(true) selects float pair
 // arithmetic with 64-bit fixed-point accumulation; setPrecision picks any of the modes of md_precision
-// (include/md_b200.h): FixedDouble is exact fixed-point separations with double pair terms (MD_PREC_FX64).
+// (include/md_b200.h): FixedDouble is exact fixed-point separations with double pair terms (MD_PREC_FX64),
+// FixedMixed the same separations with float pair terms and double ones for the close pairs (MD_PREC_FX32).
 
 #include "NeighbourList.hpp"
 #include "System.hpp"
@@ -12,7 +13,7 @@ struct md_forcefield;
 
 class LennardJonesForceField {
 public:
-    enum class Precision { Double = 0, FloatFixedPoint = 1, Float = 2, FixedDouble = 3 };
+    enum class Precision { Double = 0, FloatFixedPoint = 1, Float = 2, FixedDouble = 3, FixedMixed = 4 };
 
     LennardJonesForceField(double epsilon, double sigma, double cut_off);
     ~LennardJonesForceField();

@@ -17,7 +17,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmdgpu.so")
 
-PREC_FP64, PREC_FP32FX, PREC_FP32, PREC_FX64 = 0, 1, 2, 3
+PREC_FP64, PREC_FP32FX, PREC_FP32, PREC_FX64, PREC_FX32 = 0, 1, 2, 3, 4
+GRAPH_EXACT_TILES = 1  # md_system_set_graph test flag
 _ERRORS = {1: "MD_ERR_INVALID", 2: "MD_ERR_CUTOFF", 3: "MD_ERR_LIST_RADIUS", 4: "MD_ERR_NO_REVERSE_INDEX",
            5: "MD_ERR_CAPACITY", 6: "MD_ERR_CUDA", 7: "MD_ERR_NO_DEVICE", 8: "MD_ERR_STATE", 9: "MD_ERR_TIMEOUT"}
 
@@ -75,6 +76,9 @@ def _load():
         "md_forces_list": (_I, [_P, _P, _P, _PD, _PD, _PD]), "md_forces_all_pairs": (_I, [_P, _P, _PD, _PD, _PD]),
         "md_step_list": (_I, [_P, _P, _P, _D, _PD, _PI]), "md_step_all_pairs": (_I, [_P, _P, _D, _PD]),
         "md_run": (_I, [_P, _P, _P, _D, _I64, C.POINTER(md_run_options), _PD, _PD, _PD]),
+        "md_run_prepare": (_I, [_P, _P, _P, _D, _I64, C.POINTER(md_run_options), _I]),
+        "md_system_set_graph": (_I, [_P, _I, _I]),
+        "md_system_graph_info": (_I, [_P, C.POINTER(_I), _PU64, _PU64, _PU64]),
         "md_rdf_create": (_I, [_D, _I, _PP]), "md_rdf_destroy": (_I, [_P]), "md_rdf_sample": (_I, [_P, _P, _P]),
         "md_rdf_values": (_I, [_P, _PD, _PD, _PI]), "md_rdf_histogram": (_I, [_P, _PD]),
         "md_fcc_lattice": (_I, [_I, _D, _PD]), "md_initialize_velocities": (_I, [_P, _D, C.c_uint32]),
@@ -87,6 +91,8 @@ def _load():
                                  C.POINTER(md_batch_options), _PP]),
         "md_batch_destroy": (_I, [_P]), "md_batch_info": (_I, [_P, _PI, C.POINTER(C.c_int64), _PI, _PU64]),
         "md_batch_stream": (_I, [_P, _PP]), "md_batch_run": (_I, [_P, _I64, _PD, _PD, _PD]),
+        "md_batch_run_records": (_I, [_P, _I64, _PD, _PD, _PD, _PD]),
+        "md_batch_set_thermostat": (_I, [_P, _I, _I, _D, _PD, _PU64]),
         "md_batch_energy": (_I, [_P, _PD, _PD, _PD, _PD]),
         "md_batch_download": (_I, [_P, _I, _PD, _PD, _PD, _PD, _PU64]),
         "md_batch_state_hash": (_I, [_P, _PU64]), "md_batch_rebuilds": (_I, [_P, _PU64]),
@@ -277,6 +283,16 @@ class System:
         x = C.c_uint64()
         _check(LIB.md_system_launch_count(self.h, C.byref(x)))
         return x.value
+
+    def set_graph(self, chunk_steps: int, exact_tiles: bool = False):
+        """md_run's CUDA-graph chunk length (0: every step from the host); exact_tiles is a test switch that makes
+        device rebuilds outgrow the recorded tile so chunks rerun on the host path (md_system_set_graph)."""
+        _check(LIB.md_system_set_graph(self.h, chunk_steps, GRAPH_EXACT_TILES if exact_tiles else 0))
+
+    def graph_info(self) -> dict:
+        c, g, l, r = C.c_int(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(LIB.md_system_graph_info(self.h, C.byref(c), C.byref(g), C.byref(l), C.byref(r)))
+        return {"chunk_steps": c.value, "graphs": g.value, "launches": l.value, "recoveries": r.value}
 
     def profile(self, enable: bool):
         _check(LIB.md_profile_enable(self.h, int(enable)))
@@ -509,6 +525,31 @@ class VelocityVerletIntegrator:
             bussi_tau: float = 0.5, bussi_r1=None, bussi_chi2=None, rdf: RadialDistribution | None = None,
             rdf_every: int = 10, first_step: int = 1, record: bool = True):
         """n_steps device-resident steps (md_run). Returns per-step (pe, ke, virial) arrays when record."""
+        o, keep = self._options(thermostat, rescale_every, rescale_temperature, melt_until, melt_temperature,
+                                bussi_temperature, bussi_tau, bussi_r1, bussi_chi2, rdf, rdf_every, first_step)
+        pe = np.zeros(n_steps) if record else None
+        ke = np.zeros(n_steps) if record else None
+        w = np.zeros(n_steps) if record else None
+        _check(LIB.md_run(system.h, force_field.h, neighbour_list.h, self.dt, n_steps, C.byref(o), _pd(pe), _pd(ke),
+                          _pd(w)))
+        neighbour_list.n = system.n
+        return pe, ke, w
+
+    def prepare(self, system: System, force_field: LennardJonesForceField, neighbour_list: NeighbourList,
+                n_steps: int, thermostat: str = "none", rescale_every: int = 10, rescale_temperature: float = 0.0,
+                melt_until: int = 0, melt_temperature: float = 2.0, bussi_temperature: float = 0.0,
+                bussi_tau: float = 0.5, rdf: RadialDistribution | None = None, rdf_every: int = 10,
+                first_step: int = 1, record: bool = True):
+        """Capture the CUDA graphs run() would launch with these arguments, without running (md_run_prepare)."""
+        r1 = np.zeros(max(n_steps, 1))
+        o, keep = self._options(thermostat, rescale_every, rescale_temperature, melt_until, melt_temperature,
+                                bussi_temperature, bussi_tau, r1, r1, rdf, rdf_every, first_step)
+        _check(LIB.md_run_prepare(system.h, force_field.h, neighbour_list.h, self.dt, n_steps, C.byref(o),
+                                  3 if record else 0))
+
+    @staticmethod
+    def _options(thermostat, rescale_every, rescale_temperature, melt_until, melt_temperature, bussi_temperature,
+                 bussi_tau, bussi_r1, bussi_chi2, rdf, rdf_every, first_step):
         o = md_run_options()
         o.thermostat = {"none": 0, "rescale": 1, "bussi": 2}[thermostat]
         o.rescale_every = rescale_every
@@ -526,13 +567,7 @@ class VelocityVerletIntegrator:
         o.rdf = rdf.h if rdf is not None else None
         o.rdf_every = rdf_every
         o.first_step = first_step
-        pe = np.zeros(n_steps) if record else None
-        ke = np.zeros(n_steps) if record else None
-        w = np.zeros(n_steps) if record else None
-        _check(LIB.md_run(system.h, force_field.h, neighbour_list.h, self.dt, n_steps, C.byref(o), _pd(pe), _pd(ke),
-                          _pd(w)))
-        neighbour_list.n = system.n
-        return pe, ke, w
+        return o, keep
 
 
 class Batch:
@@ -580,16 +615,26 @@ class Batch:
         _check(LIB.md_batch_info(self.h, C.byref(r), C.byref(atoms), C.byref(cap), C.byref(launches)))
         return dict(replicas=r.value, atoms=atoms.value, capacity=cap.value, launches=launches.value)
 
-    def run(self, n_steps: int):
+    def run(self, n_steps: int, record: bool = True, inside: bool = False):
         """n_steps steps of every replica; returns (pe, virial, ke) arrays of shape (n_steps // energy_every,
-        replicas) when energy_every > 0, else None."""
-        rows = n_steps // self.energy_every if self.energy_every > 0 else 0
+        replicas) when energy_every > 0 and record, plus the inside-cutoff pair counts with inside, else None."""
+        rows = n_steps // self.energy_every if self.energy_every > 0 and record else 0
         if rows == 0:
             _check(LIB.md_batch_run(self.h, n_steps, None, None, None))
             return None
-        pe, w, ke = (np.zeros((rows, self.replicas)) for _ in range(3))
-        _check(LIB.md_batch_run(self.h, n_steps, _pd(pe), _pd(w), _pd(ke)))
-        return pe, w, ke
+        pe, w, ke, ins = (np.zeros((rows, self.replicas)) for _ in range(4))
+        _check(LIB.md_batch_run_records(self.h, n_steps, _pd(pe), _pd(w), _pd(ke), _pd(ins) if inside else None))
+        return (pe, w, ke, ins) if inside else (pe, w, ke)
+
+    def set_thermostat(self, thermostat: str, temperatures=None, rescale_every: int = 10, bussi_tau: float = 0.5,
+                       seeds=None):
+        """Switch the thermostat between runs (md_batch_set_thermostat): "none", "rescale" (every rescale_every
+        steps to temperatures[r]) or "bussi" (coupling time bussi_tau, generators started afresh from seeds)."""
+        temps = None if temperatures is None else np.ascontiguousarray(temperatures, dtype=np.float64)
+        sd = None if seeds is None else np.ascontiguousarray(seeds, dtype=np.uint64)
+        self.thermostat = thermostat
+        _check(LIB.md_batch_set_thermostat(self.h, {"none": 0, "rescale": 1, "bussi": 2}[thermostat], rescale_every,
+                                           bussi_tau, _pd(temps), _pu(sd)))
 
     def energy(self):
         """(pe, virial, ke, inside) arrays over replicas for the current state."""

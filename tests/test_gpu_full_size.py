@@ -1,8 +1,9 @@
 """The list path at the headline size, N = 4,000,000 (FCC 100^3 x 4, density 0.8442), through properties that do
 not need the oracle to run at that size: every force-kernel variant and both list builds give the same bits, the
 FP64 forces sum to zero (tests/test_forcefield.cpp:103-119), and the reduced-precision modes stay within their
-error bounds of the FP64 path (FX64: every particle within 1e-6 of the rms force; FP32FX: the reference's
-mixed-precision tolerance, tests/test_forcefield.cpp:123-149). The state is a liquid: 60 steps of the bench's
+error bounds of the FP64 path (FX64 and FX32: every particle within 1e-6 of the rms force and 99 % of particles
+within 1e-6 of their own force; FP32FX: the reference's mixed-precision tolerance,
+tests/test_forcefield.cpp:123-149). The state is a liquid: 60 steps of the bench's
 melt/rescale schedule from the lattice.
 """
 from __future__ import annotations
@@ -76,3 +77,21 @@ def test_reduced_precision_within_bounds_of_fp64(md, liquid_4m):
     f32, pe32, w32, in32, _ = forces(md, liquid_4m, md.PREC_FP32FX)
     assert np.abs(f32 - f64).max() < 1e-5 * np.abs(f64).max()
     assert abs(pe32 - pe64) < 1e-5 * abs(pe64) and abs(w32 - w64) < 1e-4 * abs(w64) and in32 == in64
+
+
+def test_fx32_meets_the_per_particle_bound_at_4m(md, liquid_4m):
+    """MD_PREC_FX32 at the headline size: max |dF_i| <= 1e-6 rms |F| and >= 99 % of particles with
+    |dF_i| <= 1e-6 |F_i| against the FP64 path, PE within 1e-6 and the virial within 1e-5 relative, the same
+    inside count, and a bit-identical repeat."""
+    f64, pe64, w64, in64, _ = forces(md, liquid_4m, md.PREC_FP64)
+    f, pe, w, ins, _ = forces(md, liquid_4m, md.PREC_FX32)
+    d = np.sqrt(((f - f64) ** 2).sum(axis=0))
+    mag = np.sqrt((f64 ** 2).sum(axis=0))
+    rms = float(np.sqrt((mag ** 2).mean()))
+    frac = float((d <= 1e-6 * mag).mean())
+    print("fx32 4M: max|dF|/rms", d.max() / rms, "frac<=1e-6", frac, "pe", abs(pe - pe64) / abs(pe64),
+          "w", abs(w - w64) / abs(w64))
+    assert d.max() <= 1e-6 * rms and frac >= 0.99
+    assert abs(pe - pe64) < 1e-6 * abs(pe64) and abs(w - w64) < 1e-5 * abs(w64) and ins == in64
+    f2, pe2, w2, ins2, _ = forces(md, liquid_4m, md.PREC_FX32)
+    assert np.array_equal(f, f2) and (pe2, w2, ins2) == (pe, w, ins)

@@ -85,12 +85,14 @@ def test_md_sim_reordered_paths_within_tolerance(golden, tmp_path, case, rtol):
     assert out["result"]["rebuilds"] == g["result"]["rebuilds"]
 
 
-# --precision fx64 (exact fixed-point separations, double pair terms, 64-bit fixed-point sums): the per-particle
-# force error against FP64 is about 2e-7 of the rms force, so the observables of the reference's own
-# --deterministic run on the same command line stay within 2e-6 of their largest magnitude over 400 steps
-def test_md_sim_fx64_within_bound_of_reference_deterministic(golden, tmp_path):
+# --precision fx64 (exact fixed-point separations, double pair terms, 64-bit fixed-point sums) and fx32 (the same
+# with float pair terms except for the close pairs): the per-particle force error against FP64 is about 2e-7 of
+# the rms force, so the observables of the reference's own --deterministic run on the same command line stay
+# within 2e-6 of their largest magnitude over 400 steps
+@pytest.mark.parametrize("prec", ["fx64", "fx32"])
+def test_md_sim_fixed_point_within_bound_of_reference_deterministic(golden, tmp_path, prec):
     g = golden["nve_rescale"]
-    out = run_md_sim([*g["args"], "--precision", "fx64"], str(tmp_path))
+    out = run_md_sim([*g["args"], "--precision", prec], str(tmp_path))
     ref, got = csv_columns(g["files"]["csv"]), csv_columns(out["files"]["csv"])
     assert got.shape == ref.shape
     assert np.array_equal(got[:, 0], ref[:, 0])

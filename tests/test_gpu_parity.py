@@ -234,12 +234,14 @@ def test_total_force_and_momentum(md, golden):
     assert np.all(np.abs(p) < 1e-10)
 
 
+@pytest.mark.parametrize("prec", ["PREC_FX64", "PREC_FX32"])
 @pytest.mark.parametrize("cells,density", [(8, 0.8442), (6, 0.5), (20, 1.0)])
-def test_fx64_per_particle_force_error(md, golden, cells, density):
-    """MD_PREC_FX64 (exact fixed-point separations, double pair terms): every particle's force within 1e-6 of
-    the rms force of the FP64 path, 99 % of particles within 1e-6 of their own force, PE and virial within 1e-9,
-    the same inside count, bit-identical repeats. Liquid states (config 1's after 1000 steps, and melted
-    boxes), plus the FCC lattice start."""
+def test_fixed_point_modes_per_particle_force_error(md, golden, cells, density, prec):
+    """MD_PREC_FX64 (exact fixed-point separations, double pair terms) and MD_PREC_FX32 (the same separations,
+    float pair terms except for the close pairs, which are double): every particle's force within 1e-6 of the rms
+    force of the FP64 path, 99 % of particles within 1e-6 of their own force, PE and virial close to FP64's
+    (FX64 within 5e-8 relative; FX32 within 1e-6 and 1e-5: its float pair energies round at ~6e-8 each), the same
+    inside count, bit-identical repeats. Melted liquid states (config 1's after 1000 steps, and melted boxes)."""
     if cells == 8:
         s, nl = liquid(md, golden)
     else:
@@ -252,28 +254,33 @@ def test_fx64_per_particle_force_error(md, golden, cells, density):
     ff = md.LennardJonesForceField(1.0, 1.0, 2.5)
     pe64 = ff.compute_forces(s, nl)
     f64, w64, ins64 = s.forces(), ff.virial, ff.inside_pairs
-    ff.set_precision(md.PREC_FX64)
+    ff.set_precision(getattr(md, prec))
     pe = ff.compute_forces(s, nl)
     f = s.forces()
     d = np.linalg.norm(f - f64, axis=0)
     mag = np.linalg.norm(f64, axis=0)
     rms = np.sqrt((mag ** 2).mean())
+    print(prec, cells, density, "max|dF|/rms", d.max() / rms, "frac<=1e-6", (d <= 1e-6 * mag).mean(),
+          "pe", abs(pe - pe64) / abs(pe64), "w", abs(ff.virial - w64) / abs(w64))
     assert d.max() <= 1e-6 * rms, d.max() / rms
     assert (d <= 1e-6 * mag).mean() >= 0.99, (d <= 1e-6 * mag).mean()
-    # frames quantised to 2^-28 put ~4e-9 on each separation: PE and virial agree to a few 1e-9 relative
-    assert abs(pe - pe64) <= 5e-8 * abs(pe64) and abs(ff.virial - w64) <= 5e-8 * abs(w64)
+    if prec == "PREC_FX64":
+        # frames quantised to 2^-28 put ~4e-9 on each separation: PE and virial agree to a few 1e-9 relative
+        assert abs(pe - pe64) <= 5e-8 * abs(pe64) and abs(ff.virial - w64) <= 5e-8 * abs(w64)
+    else:
+        assert abs(pe - pe64) <= 1e-6 * abs(pe64) and abs(ff.virial - w64) <= 1e-5 * abs(w64)
     assert ff.inside_pairs == ins64
     assert ff.compute_forces(s, nl) == pe and np.array_equal(s.forces(), f)
 
 
-@pytest.mark.parametrize("prec", ["fp64", "fp32fx", "fp32", "fx64"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32fx", "fp32", "fx64", "fx32"])
 def test_nve_energy_drift(md, golden, prec):
     """tests/test_dynamics.cpp:40-56 and tests/test_forcefield.cpp:151-167: |dE/E0| < 3e-4 over 2000 steps
     with more than one rebuild, starting from a melted liquid."""
     s, nl = liquid(md, golden)
     ff = md.LennardJonesForceField(1.0, 1.0, C1["rc"],
                                    precision={"fp64": md.PREC_FP64, "fp32fx": md.PREC_FP32FX, "fp32": md.PREC_FP32,
-                                              "fx64": md.PREC_FX64}[prec])
+                                              "fx64": md.PREC_FX64, "fx32": md.PREC_FX32}[prec])
     pe0 = ff.compute_forces(s, nl)
     e0 = s.kinetic_energy() + pe0
     integ = md.VelocityVerletIntegrator(C1["dt"])
@@ -548,7 +555,7 @@ def test_list_build_variants_agree(md, cells, density, temperature, skin):
             assert np.array_equal(d[k], out[0][3][k]), k
 
 
-@pytest.mark.parametrize("prec", ["PREC_FP32FX", "PREC_FP32", "PREC_FX64"])
+@pytest.mark.parametrize("prec", ["PREC_FP32FX", "PREC_FP32", "PREC_FX64", "PREC_FX32"])
 def test_fused_next_drift_matches_separate_steps(md, prec):
     """md_run fuses each NVE step's closing kick with the next step's opening kick and drift in the float and FX64
     force kernels (new positions and frames into spare buffers, the half-skin test alongside). The trajectory, its

@@ -1,5 +1,5 @@
 """Precision sweep on the 256,000-atom FCC start (40^3 x 4) over densities {0.5, 0.8442, 1.0} and
-T* in {0.71, 1.5, 3.0}: FP32 fixed-point, FP32 float-accumulate and FX64 against FP64 — per-particle force error,
+T* in {0.71, 1.5, 3.0}: FP32 fixed-point, FP32 float-accumulate, FX64 and FX32 against FP64 — per-particle force error,
 energy drift, virial pressure and g(r). The full-length sweep (10,000 steps) is `bench.py --sweep precision`;
 here 400 steps per run keep the test to a few minutes, with the tolerances stated below."""
 from __future__ import annotations
@@ -30,9 +30,11 @@ def test_precision_sweep_short(md):
             assert abs(run["pressure"] - ref["pressure"]) <= 0.02 * abs(ref["pressure"]) + 0.01, (tag, prec)
             assert run["max_dg_vs_fp64"] < 0.1, (tag, prec, run["max_dg_vs_fp64"])
         assert pt["fp64"]["max_drift"] < 3e-4, (tag, pt["fp64"])
-        # FX64: exact separations and double pair terms meet the 1e-6 per-particle bound
-        e = pt["force_error_vs_fp64"]["fx64"]
-        assert e["max_particle_dF_over_rms_F"] <= 1e-6 and e["frac_particles_rel_le_1e-6"] >= 0.99, (tag, e)
-        run, ref = pt["fx64"], pt["fp64"]
-        assert run["max_drift"] < max(3e-4, 10 * ref["max_drift"]), (tag, run, ref)
-        assert abs(run["pressure"] - ref["pressure"]) <= 0.02 * abs(ref["pressure"]) + 0.01, tag
+        # FX64 (exact separations, double pair terms) and FX32 (the same separations, double terms for the close
+        # pairs only) meet the 1e-6 per-particle bound
+        for prec in ("fx64", "fx32"):
+            e = pt["force_error_vs_fp64"][prec]
+            assert e["max_particle_dF_over_rms_F"] <= 1e-6 and e["frac_particles_rel_le_1e-6"] >= 0.99, (tag, prec, e)
+            run, ref = pt[prec], pt["fp64"]
+            assert run["max_drift"] < max(3e-4, 10 * ref["max_drift"]), (tag, prec, run, ref)
+            assert abs(run["pressure"] - ref["pressure"]) <= 0.02 * abs(ref["pressure"]) + 0.01, (tag, prec)
