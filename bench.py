@@ -65,6 +65,8 @@ def args_parse():
     p.add_argument("--sweep", choices=["precision"], default=None,
                    help="instead of the headline line: the N=256,000 precision sweep over densities {0.5, 0.8442, 1.0} "
                         "x T {0.71, 1.5, 3.0} (one JSON line per state point; --steps NVE steps each)")
+    p.add_argument("--sweep-replicas", type=int, default=4,
+                   help="replicas per state point of the precision sweep (error bars from their spread)")
     p.add_argument("--nist", action="store_true",
                    help="instead of the headline line: the reference's NIST validation (bench/validate.py: 16 state "
                         "points x 8 replicas of 500 atoms, 10,000 + 20,000 steps) in one md_batch, one JSON line per "
@@ -617,54 +619,87 @@ def run_gpu_arm(a):
 # ---- precision sweep (the N = 256,000 density x temperature grid) -------------------------------------------
 
 def precision_sweep(cells=40, densities=(0.5, 0.8442, 1.0), temperatures=(0.71, 1.5, 3.0), steps=10000,
-                    equil=200, rdf_every=100, device=0):
-    """For each state point: melt/rescale equilibration (T = 2 for the first third, then T, every 10 steps),
-    force errors of the float modes against FP64 on the equilibrated state, then `steps` NVE steps from that
-    same state in each precision. Yields one dict per state point: per-particle force errors, energy drift
-    (max |E - E0| / |E0| and its per-step slope), mean virial pressure P = (2K + W) / 3V, the largest g(r)
-    difference from the FP64 run (g(r) from the run's list pairs to r_c every `rdf_every` steps) and
-    atom-steps/s."""
+                    equil=200, rdf_every=100, device=0, replicas=4):
+    """For each state point and each of `replicas` replicas (FCC start with velocities from seed 42 + r): the
+    melt/rescale equilibration in FP64 (T = 2 for the first third, then T, every 10 steps), then `steps` NVE steps
+    from that replica's equilibrated state in each precision. Force errors of the float modes against FP64 are
+    taken on replica 0's equilibrated state. Yields one dict per state point; per precision the replica means and
+    standard errors of the energy drift (max |E - E0| / |E0| and the per-step slope), the mean virial pressure
+    P = (2K + W) / 3V and atom-steps/s, g(r) from the run's list pairs to r_c every `rdf_every` steps, and against
+    FP64, replica by replica (each pair of runs starts from the same state): the mean pressure difference with its
+    standard error and z-score, and the largest g(r) difference of the replica-mean g(r) in units of the replica
+    standard error of that bin."""
     import numpy as np
 
     import mdgpu as md
 
+    names = ("fp64", "fp32fx", "fp32", "fx64", "fx32")
     for rho in densities:
         for temp in temperatures:
-            s = md.fcc_system(cells, rho, temp, seed=42, device=device)
-            nl = md.NeighbourList(2.5, 0.3)
-            ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=md.PREC_FP64)
-            integ = md.VelocityVerletIntegrator(0.005)
-            nl.build(s)
-            ff.compute_forces(s, nl)
-            integ.run(s, ff, nl, equil, thermostat="rescale", rescale_every=10, rescale_temperature=temp,
-                      melt_until=equil // 3, melt_temperature=2.0, record=False)
-            errors = force_errors(md, s, nl)
-            start = s.download()
-            vol = s.box ** 3
-            runs = {}
-            for name in ("fp64", "fp32fx", "fp32", "fx64", "fx32"):
-                prec = PRECISIONS[name][0]
-                r = md.System.from_arrays(start["pos"], s.box, vel=start["vel"], force=start["force"], device=device)
-                rl = md.NeighbourList(2.5, 0.3)
-                rf = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)
-                rl.build(r)
-                pe0 = rf.compute_forces(r, rl)
-                e0 = r.kinetic_energy() + pe0
-                rdf = md.RadialDistribution(2.5, 100)
-                t0 = time.perf_counter()
-                pe, ke, w = integ.run(r, rf, rl, steps, rdf=rdf, rdf_every=rdf_every)
-                dt = time.perf_counter() - t0
-                e = pe + ke
-                dev = np.abs((e - e0) / e0)
-                slope = float(np.polyfit(np.arange(1, steps + 1), (e - e0) / abs(e0), 1)[0])
-                runs[name] = {"max_drift": float(dev.max()), "drift_per_step": slope,
-                              "pressure": float(np.mean((2.0 * ke + w) / (3.0 * vol))),
-                              "g": rdf.values(), "atom_steps_per_s": r.n * steps / dt, "rebuilds": rl.rebuild_count}
-            out = {"density": rho, "temperature": temp, "n_atoms": s.n, "steps": steps, "force_error_vs_fp64": errors}
-            g_ref = runs["fp64"]["g"]
-            for name, rr in runs.items():
-                rr["max_dg_vs_fp64"] = float(np.abs(rr.pop("g") - g_ref).max())
-                out[name] = rr
+            runs = {name: [] for name in names}
+            errors = None
+            n_atoms = 0
+            for rep in range(replicas):
+                s = md.fcc_system(cells, rho, temp, seed=42 + rep, device=device)
+                nl = md.NeighbourList(2.5, 0.3)
+                ff = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=md.PREC_FP64)
+                integ = md.VelocityVerletIntegrator(0.005)
+                nl.build(s)
+                ff.compute_forces(s, nl)
+                integ.run(s, ff, nl, equil, thermostat="rescale", rescale_every=10, rescale_temperature=temp,
+                          melt_until=equil // 3, melt_temperature=2.0, record=False)
+                if rep == 0:
+                    errors = force_errors(md, s, nl)
+                start = s.download()
+                vol = s.box ** 3
+                n_atoms = s.n
+                for name in names:
+                    prec = PRECISIONS[name][0]
+                    r = md.System.from_arrays(start["pos"], s.box, vel=start["vel"], force=start["force"],
+                                              device=device)
+                    rl = md.NeighbourList(2.5, 0.3)
+                    rf = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)
+                    rl.build(r)
+                    pe0 = rf.compute_forces(r, rl)
+                    e0 = r.kinetic_energy() + pe0
+                    rdf = md.RadialDistribution(2.5, 100)
+                    t0 = time.perf_counter()
+                    pe, ke, w = integ.run(r, rf, rl, steps, rdf=rdf, rdf_every=rdf_every)
+                    dt = time.perf_counter() - t0
+                    e = pe + ke
+                    dev = np.abs((e - e0) / e0)
+                    slope = float(np.polyfit(np.arange(1, steps + 1), (e - e0) / abs(e0), 1)[0])
+                    runs[name].append({"max_drift": float(dev.max()), "drift_per_step": slope,
+                                       "pressure": float(np.mean((2.0 * ke + w) / (3.0 * vol))), "g": rdf.values(),
+                                       "atom_steps_per_s": r.n * steps / dt, "rebuilds": rl.rebuild_count})
+            out = {"density": rho, "temperature": temp, "n_atoms": n_atoms, "steps": steps, "replicas": replicas,
+                   "force_error_vs_fp64": errors}
+
+            def mean_se(x):
+                x = np.asarray(x, dtype=np.float64)
+                return float(x.mean()), (float(x.std(ddof=1) / np.sqrt(len(x))) if len(x) > 1 else None)
+
+            g_ref = np.array([r["g"] for r in runs["fp64"]])
+            for name in names:
+                rr = runs[name]
+                row = {}
+                for key in ("max_drift", "drift_per_step", "pressure", "atom_steps_per_s", "rebuilds"):
+                    row[key], row[key + "_err"] = mean_se([r[key] for r in rr])
+                g = np.array([r["g"] for r in rr])
+                row["max_dg_vs_fp64"] = float(np.abs(g.mean(axis=0) - g_ref.mean(axis=0)).max())
+                if replicas > 1 and name != "fp64":
+                    dp = [a["pressure"] - b["pressure"] for a, b in zip(rr, runs["fp64"])]
+                    m, se = mean_se(dp)
+                    row["dp_vs_fp64"], row["dp_vs_fp64_err"] = m, se
+                    row["z_pressure_vs_fp64"] = m / se if se else None
+                    dg = g - g_ref
+                    se_g = dg.std(axis=0, ddof=1) / np.sqrt(replicas)
+                    mask = se_g > 0
+                    row["max_abs_z_g_vs_fp64"] = (float(np.abs(dg.mean(axis=0)[mask] / se_g[mask]).max())
+                                                  if mask.any() else None)
+                    dd = [a["max_drift"] - b["max_drift"] for a, b in zip(rr, runs["fp64"])]
+                    row["d_drift_vs_fp64"], row["d_drift_vs_fp64_err"] = mean_se(dd)
+                out[name] = row
             yield out
 
 
@@ -685,7 +720,7 @@ def main():
                         "prod_steps": nist.PROD_STEPS, "batch_atoms": info["atoms"], "wall_s": wall})
             print(json.dumps(row), flush=True)
     elif a.sweep == "precision":
-        for line in precision_sweep(steps=a.steps):
+        for line in precision_sweep(steps=a.steps, replicas=a.sweep_replicas):
             print(json.dumps(line), flush=True)
     else:
         run_gpu_arm(a)

@@ -172,10 +172,14 @@ md_status forces_list_fx32_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
     const int n = static_cast<int>(s->n);
     const bool kick = kick_dt > 0.0;
     const Fx64LJ dlj = fx64_lj(ff);
+    // the float path works in frame units (2^-28): sigma^2, r_c^2 and the band scaled by 2^56. The float r^2 of
+    // an exact separation rounded once per component is within ~6e-7 of r^2 (relative): a shell of 1e-5 r_c^2
+    // holds every pair whose float and exact cutoff tests could disagree
     FloatLJ flj = float_lj(ff);
-    // the float r^2 of an exact separation rounded once per component is within ~6e-7 of r^2 (relative): a
-    // shell of 1e-5 r_c^2 holds every pair whose float and exact cutoff tests could disagree
-    flj.band = static_cast<float>(1e-5 * ff->lj.rc2);
+    constexpr double kFrameArea = kFrameScale * kFrameScale;  // 2^56
+    flj.sig2 = static_cast<float>(ff->lj.sig2 * kFrameArea);
+    flj.rc2 = static_cast<float>(ff->lj.rc2 * kFrameArea);
+    flj.band = static_cast<float>(1e-5 * ff->lj.rc2 * kFrameArea);
     MD_CUDA(ff->fx_acc.reserve(4));
     if (want_energy || kick) MD_CUDA(cudaMemsetAsync(ff->fx_acc.p, 0, 4 * sizeof(long long), s->stream));
     auto* acc = reinterpret_cast<unsigned long long*>(ff->fx_acc.p);

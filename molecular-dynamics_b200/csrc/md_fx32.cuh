@@ -60,7 +60,9 @@ __global__ void k_rows_near_first(const double4* __restrict__ ref_pos, int n, Bo
 }
 
 // One 8-entry group in float from fixed-point frames: the exact integer separation (q_i - q_j) + offset, each
-// component rounded once to float (__int2float_rn, then the exact scaling by 2^-28), then float_pair. Pairs in
+// component rounded once to float (__int2float_rn) and kept in frame units, then float_pair with constants in
+// frame units (frame_units_lj): r^2 and 1/r^2 are the length-unit values times 2^56 and 2^-56 exactly, the pair's
+// F/r times 2^-56 and its force times 2^-28, its energy and virial unchanged. Pairs in
 // the shell around r_c where the float r^2 could misclassify them are flagged through *shell; the caller then runs
 // the group again with kExact, where the reference's exact double test decides them (the same operations in the
 // same order either way).
@@ -83,9 +85,11 @@ __device__ __forceinline__ GroupSums fx32_float_group(const uint4& e0, const uin
         const int sx = static_cast<int>(static_cast<unsigned>(qi.x) - static_cast<unsigned>(qj.x) + static_cast<unsigned>(oxy.x));
         const int sy = static_cast<int>(static_cast<unsigned>(qi.y) - static_cast<unsigned>(qj.y) + static_cast<unsigned>(oxy.y));
         const int sz = static_cast<int>(static_cast<unsigned>(qi.z) - static_cast<unsigned>(qj.z) + static_cast<unsigned>(s_z[code]));
-        const float dx = __fmul_rn(__int2float_rn(sx), static_cast<float>(kFrameUnit));
-        const float dy = __fmul_rn(__int2float_rn(sy), static_cast<float>(kFrameUnit));
-        const float dz = __fmul_rn(__int2float_rn(sz), static_cast<float>(kFrameUnit));
+        // in frame units (2^-28): lj holds sigma^2, r_c^2 and the band scaled by 2^56, so every product below
+        // has the mantissa it would have in length units, scaled by an exact power of two
+        const float dx = __int2float_rn(sx);
+        const float dy = __int2float_rn(sy);
+        const float dz = __int2float_rn(sz);
         const float r2 = fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
         bool in = !pad && r2 < lj.rc2;
         const bool near = !pad && fabsf(r2 - lj.rc2) < lj.band;
@@ -162,7 +166,7 @@ __global__ void __launch_bounds__(128) k_force_fx32(const int4* __restrict__ fra
                 GroupSums gs =
                     fx32_float_group<kEnergy, false>(e0, e1, qi, frames, s_xy, s_z, pos, i, box, flj, gin, &shell);
                 if (shell) gs = fx32_float_group_exact<kEnergy>(e0, e1, qi, frames, s_xy, s_z, pos, i, box, flj, &gin);
-                a.add_group_fine(gs.x, gs.y, gs.z, gs.e, gs.w, e_fx, w_fx);
+                a.add_group_frame(gs.x, gs.y, gs.z, gs.e, gs.w, e_fx, w_fx);
             }
             ins += gin;
         }

@@ -1,7 +1,8 @@
 """Precision sweep on the 256,000-atom FCC start (40^3 x 4) over densities {0.5, 0.8442, 1.0} and
 T* in {0.71, 1.5, 3.0}: FP32 fixed-point, FP32 float-accumulate, FX64 and FX32 against FP64 — per-particle force error,
-energy drift, virial pressure and g(r). The full-length sweep (10,000 steps) is `bench.py --sweep precision`;
-here 400 steps per run keep the test to a few minutes, with the tolerances stated below."""
+energy drift, virial pressure and g(r), each a mean over replicas with its standard error. The full-length sweep
+(10,000 steps, 4 replicas) is `bench.py --sweep precision`; here 400 steps per run and 2 replicas keep the test to
+a few minutes, with the tolerances stated below."""
 from __future__ import annotations
 
 import pytest
@@ -12,7 +13,7 @@ pytestmark = pytest.mark.gpu
 def test_precision_sweep_short(md):
     import bench
 
-    for pt in bench.precision_sweep(steps=400, equil=100):
+    for pt in bench.precision_sweep(steps=400, equil=100, replicas=2):
         tag = (pt["density"], pt["temperature"])
         for prec in ("fp32fx", "fp32"):
             e = pt["force_error_vs_fp64"][prec]
@@ -30,6 +31,9 @@ def test_precision_sweep_short(md):
             assert abs(run["pressure"] - ref["pressure"]) <= 0.02 * abs(ref["pressure"]) + 0.01, (tag, prec)
             assert run["max_dg_vs_fp64"] < 0.1, (tag, prec, run["max_dg_vs_fp64"])
         assert pt["fp64"]["max_drift"] < 3e-4, (tag, pt["fp64"])
+        # replica error bars: every float mode reports its paired pressure difference from FP64 with an error
+        for prec in ("fp32fx", "fp32", "fx64", "fx32"):
+            assert pt[prec]["dp_vs_fp64_err"] is not None and pt[prec]["pressure_err"] is not None, (tag, prec)
         # FX64 (exact separations, double pair terms) and FX32 (the same separations, double terms for the close
         # pairs only) meet the 1e-6 per-particle bound
         for prec in ("fx64", "fx32"):
