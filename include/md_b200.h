@@ -211,7 +211,8 @@ md_status md_step_all_pairs(md_system* s, md_forcefield* ff, double dt, double* 
  * thermostat; then the optional g(r) sample. Outputs (each NULL or n_steps long, host memory): pe[k] the step's
  * PE, ke[k] the kinetic energy after the thermostat, virial[k].
  * The float precisions on a list with shared-memory tiles run as CUDA graphs of up to md_system_set_graph's
- * chunk length (64 steps by default): every step, the thermostat and the g(r) sample included, is in the graph,
+ * chunk length (64 steps by default) when the run is at least two chunks long or md_run_prepare captured the
+ * graphs for its length: every step, the thermostat and the g(r) sample included, is in the graph,
  * and a list rebuild is decided on the device (a conditional node runs the rebuild when the half-skin test of the
  * step's drift flagged a particle), so the host waits once per chunk. A rebuild that outgrows the row capacity or
  * the recorded shared-memory tile makes the library run that chunk again on the host path from the chunk's

@@ -171,6 +171,7 @@ struct md_system {
     DevBuf<unsigned long long> snap_hist;
     void* canon[7] = {};
     uint64_t graph_launches = 0, graph_recoveries = 0;
+    int64_t prepared_steps = -1;  // run length md_run_prepare last captured graphs for
 };
 
 void drop_run_graphs(md_system* s) {
@@ -1546,6 +1547,7 @@ md_status md_run_prepare(md_system* s, md_forcefield* ff, md_nlist* nl, double d
     ff->device = s->device;
     if (!graph_mode_ok(s, ff, nl, n_steps)) return MD_OK;  // md_run would take the host path: nothing to prepare
     MD_TRY(graph_prepare(s, ff, nl, dt, n_steps, o, (record & 1) != 0, (record & 2) != 0));
+    s->prepared_steps = n_steps;
     return sync(s);
 }
 

@@ -447,7 +447,10 @@ md_status collect_graph_profile(md_system* s, const RunGraph& g) {
 // kernel fuses with the closing kick, and recompute it after a thermostat.
 md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
                     const md_run_options& o, double* pe, double* ke, double* virial) {
-    if (graph_mode_ok(s, ff, nl, n_steps)) return run_steps_graph(s, ff, nl, dt, n_steps, o, pe, ke, virial);
+    // graphs when the run amortises their capture (two chunks or more) or md_run_prepare captured them for it
+    if (graph_mode_ok(s, ff, nl, n_steps) && (n_steps >= 2 * static_cast<int64_t>(s->graph_chunk) ||
+                                              n_steps == s->prepared_steps))
+        return run_steps_graph(s, ff, nl, dt, n_steps, o, pe, ke, virial);
     const double bussi_c = o.thermostat == 2 ? std::exp(-dt / o.bussi_tau) : 0.0;  // src/Thermostat.cpp:46
     DevBuf<double> noise;
     if (o.thermostat == 2 && n_steps > 0) {
