@@ -388,6 +388,11 @@ int initial_capacity(const md_nlist* nl, const md_system* s) {
 md_status frames_async(md_system* s, md_nlist* nl);
 CellOffsets cell_offsets(const md_nlist* nl, const md_system* s);
 
+#ifndef MD_TILE_HOME_TARGET
+#define MD_TILE_HOME_TARGET 96.0
+#endif
+constexpr double kTileHomeTarget = MD_TILE_HOME_TARGET;  // home particles per tile block aimed at
+
 // Segment length and shared-memory size of the tile kernels for this build. Segments aim at ~96 home
 // particles per block. The largest staged tile of the geometry is measured on the device (the cells only
 // change at rebuilds, so it holds until the next one); it must fit 3072 slots (96 KB of double4 for the
@@ -397,7 +402,7 @@ md_status tile_geometry(md_nlist* nl, md_system* s, bool* use) {
     const int nc = nl->grid.ncps;
     if (nc < 3 || s->n == 0) return MD_OK;
     const double avg = static_cast<double>(s->n) / (static_cast<double>(nc) * nc * nc);
-    int kk = static_cast<int>(std::lround(96.0 / std::max(avg, 1.0)));
+    int kk = static_cast<int>(std::lround(kTileHomeTarget / std::max(avg, 1.0)));
     kk = std::clamp(kk, 1, std::min(kMaxSegment, nc - 2));
     TileGeom& g = nl->tiles_geom;
     for (;;) {

@@ -22,8 +22,12 @@
 namespace md {
 
 constexpr int kTileThreads = 128;
-constexpr int kMaxSegment = 10;                      // kk <= 10 cells per segment
+#ifndef MD_TILE_MAX_SEGMENT
+#define MD_TILE_MAX_SEGMENT 10
+#endif
+constexpr int kMaxSegment = MD_TILE_MAX_SEGMENT;     // kk <= kMaxSegment cells per segment
 constexpr int kMaxStagedCells = 9 * (kMaxSegment + 2);
+constexpr int kScanPerLane = (kMaxStagedCells + 31) / 32;  // staged-cell counts per lane in tile_tables' scan
 struct TileGeom {
     int ncps;       // cells per side (>= 3)
     int kk;         // cells per segment along z
@@ -77,12 +81,12 @@ __device__ __forceinline__ void tile_tables(const TileGeom& g, const int* __rest
         t.home_end = cell_start[hc0 + kk];
     }
     __syncthreads();
-    if (threadIdx.x < 32) {  // exclusive scan of up to kMaxStagedCells counts, 4 per lane
+    if (threadIdx.x < 32) {  // exclusive scan of up to kMaxStagedCells counts, kScanPerLane per lane
         const int lane = threadIdx.x;
-        int v[4], s = 0;
+        int v[kScanPerLane], s = 0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int k = lane * 4 + q;
+        for (int q = 0; q < kScanPerLane; ++q) {
+            const int k = lane * kScanPerLane + q;
             v[q] = k < ncell ? t.count[k] : 0;
             s += v[q];
         }
@@ -93,8 +97,8 @@ __device__ __forceinline__ void tile_tables(const TileGeom& g, const int* __rest
         }
         int run = inc - s;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int k = lane * 4 + q;
+        for (int q = 0; q < kScanPerLane; ++q) {
+            const int k = lane * kScanPerLane + q;
             if (k < ncell) t.off[k] = run;
             run += v[q];
         }
