@@ -240,10 +240,10 @@ md_status md_run(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64
 md_status md_run_prepare(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps,
                          const md_run_options* opts, int record);
 /* md_run's graph chunk length (1..1024 steps; 0 runs every step from the host) and test flags:
- * MD_GRAPH_EXACT_TILES records the host's shared-memory tile bound in the graphs without headroom, so that
- * rebuilds on the device outgrow it and the chunk reruns on the host path (for tests of that path). Drops the
- * system's cached graphs. */
-#define MD_GRAPH_EXACT_TILES 1
+ * MD_GRAPH_TEST_RERUN makes every list rebuild on the device report an overflow, so that each chunk with a rebuild
+ * reruns on the host path from its starting state (for tests of that path; the results are the same bits).
+ * Drops the system's cached graphs. */
+#define MD_GRAPH_TEST_RERUN 1
 md_status md_system_set_graph(md_system* s, int chunk_steps, int flags);
 /* Graph chunk length, graphs cached, chunk graphs launched and chunks rerun on the host path. Any may be NULL. */
 md_status md_system_graph_info(const md_system* s, int* chunk_steps, uint64_t* graphs, uint64_t* launches,

@@ -1557,7 +1557,7 @@ md_status md_run_prepare(md_system* s, md_forcefield* ff, md_nlist* nl, double d
 }
 
 md_status md_system_set_graph(md_system* s, int chunk_steps, int flags) {
-    if (!s || chunk_steps < 0 || chunk_steps > 1024 || (flags & ~MD_GRAPH_EXACT_TILES))
+    if (!s || chunk_steps < 0 || chunk_steps > 1024 || (flags & ~MD_GRAPH_TEST_RERUN))
         return fail(MD_ERR_INVALID, "md_system_set_graph: bad arguments");
     MD_TRY(use_system(s));
     MD_TRY(sync(s));

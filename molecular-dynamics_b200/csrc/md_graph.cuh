@@ -40,10 +40,11 @@ __global__ void k_copy_back(int n, const double4* __restrict__ pos2, const doubl
 }
 
 // After a device-side list build: count the rebuild (state[0]) and flag a row that outgrew the capacity or a
-// staged tile that outgrew its shared memory (state[1]); the host reruns the chunk on its own path then
-__global__ void k_build_done(int* __restrict__ max_count, int cap, int* __restrict__ state) {
+// staged tile that outgrew its shared memory (state[1]); the host reruns the chunk on its own path then.
+// report_always flags every rebuild (md_system_set_graph's test flag for that path).
+__global__ void k_build_done(int* __restrict__ max_count, int cap, int* __restrict__ state, bool report_always) {
     state[0] += 1;
-    if (*max_count > cap) state[1] = 1;
+    if (*max_count > cap || report_always) state[1] = 1;
     *max_count = 0;
 }
 

@@ -142,8 +142,7 @@ md_status graph_prepare_buffers(md_system* s, md_forcefield* ff, md_nlist* nl, c
 TileGeom graph_geometry(const md_system* s, const md_nlist* nl) {
     TileGeom g = nl->tiles_geom;
     // a quarter more, rounded up to 256 slots (so a run's graphs survive small changes of the host's bound)
-    if (!(s->graph_flags & MD_GRAPH_EXACT_TILES))
-        g.max_staged = std::min(((g.max_staged + g.max_staged / 4 + 64 + 255) / 256) * 256, 12000);
+    g.max_staged = std::min(((g.max_staged + g.max_staged / 4 + 64 + 255) / 256) * 256, 12000);
     return g;
 }
 
@@ -187,7 +186,7 @@ md_status device_rebuild_async(md_system* s, md_forcefield* ff, md_nlist* nl, co
                                                                     nl->cell_sorted.p, tg, bp, cell_offsets(nl, s),
                                                                     nl->rows.p, nl->counts.p, nl->flags.p + 1);
     MD_CHECK_LAUNCH();
-    k_build_done<<<1, 1, 0, st>>>(nl->flags.p + 1, nl->cap, s->graph_state.p);
+    k_build_done<<<1, 1, 0, st>>>(nl->flags.p + 1, nl->cap, s->graph_state.p, (s->graph_flags & MD_GRAPH_TEST_RERUN) != 0);
     MD_CHECK_LAUNCH();
     if (ff->precision == MD_PREC_FX32) {
         k_rows_near_first<<<blocks_for(n, 128), 128, 0, st>>>(nl->ref_pos.p, n, s->box, nl->nf_near2, nl->rows.p,

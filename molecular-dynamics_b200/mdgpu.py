@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmdgpu.so")
 
 PREC_FP64, PREC_FP32FX, PREC_FP32, PREC_FX64, PREC_FX32 = 0, 1, 2, 3, 4
-GRAPH_EXACT_TILES = 1  # md_system_set_graph test flag
+GRAPH_TEST_RERUN = 1  # md_system_set_graph test flag
 _ERRORS = {1: "MD_ERR_INVALID", 2: "MD_ERR_CUTOFF", 3: "MD_ERR_LIST_RADIUS", 4: "MD_ERR_NO_REVERSE_INDEX",
            5: "MD_ERR_CAPACITY", 6: "MD_ERR_CUDA", 7: "MD_ERR_NO_DEVICE", 8: "MD_ERR_STATE", 9: "MD_ERR_TIMEOUT"}
 
@@ -284,10 +284,11 @@ class System:
         _check(LIB.md_system_launch_count(self.h, C.byref(x)))
         return x.value
 
-    def set_graph(self, chunk_steps: int, exact_tiles: bool = False):
-        """md_run's CUDA-graph chunk length (0: every step from the host); exact_tiles is a test switch that makes
-        device rebuilds outgrow the recorded tile so chunks rerun on the host path (md_system_set_graph)."""
-        _check(LIB.md_system_set_graph(self.h, chunk_steps, GRAPH_EXACT_TILES if exact_tiles else 0))
+    def set_graph(self, chunk_steps: int, test_rerun: bool = False):
+        """md_run's CUDA-graph chunk length (0: every step from the host); test_rerun is a test switch that makes
+        every device rebuild report an overflow, so chunks with rebuilds rerun on the host path
+        (md_system_set_graph)."""
+        _check(LIB.md_system_set_graph(self.h, chunk_steps, GRAPH_TEST_RERUN if test_rerun else 0))
 
     def graph_info(self) -> dict:
         c, g, l, r = C.c_int(), C.c_uint64(), C.c_uint64(), C.c_uint64()

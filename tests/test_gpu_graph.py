@@ -78,19 +78,20 @@ def test_graph_run_with_thermostat_and_rdf_matches_host_loop(md, prec, thermosta
 
 @pytest.mark.parametrize("prec", ["PREC_FP32FX", "PREC_FX32"])
 def test_graph_overflow_reruns_chunk_on_host_path(md, prec):
-    """With the tile bound recorded exactly (no headroom), device rebuilds outgrow it; each such chunk starts again
-    from its snapshot on the host path. The trajectory still equals the host loop's."""
+    """With the test flag, every device rebuild reports an overflow (as a row past the capacity or a cell past the
+    recorded tile would); each chunk that rebuilds starts again from its snapshot on the host path. The trajectory
+    still equals the host loop's."""
     p = getattr(md, prec)
     st, box = start(md, cells=14, temperature=1.5, seed=9)
     integ = md.VelocityVerletIntegrator(0.005)
     out = []
-    for chunk, exact in ((16, True), (0, False)):
+    for chunk, rerun in ((16, True), (0, False)):
         s, nl, ff = make(md, st, box, p)
-        s.set_graph(chunk, exact_tiles=exact)
+        s.set_graph(chunk, test_rerun=rerun)
         pe, ke, _ = integ.run(s, ff, nl, 200)
         out.append((pe, ke, s.download(), nl.rebuild_count, s.graph_info()))
     (pa, ka, sa, ra, ia), (pb, kb, sb, rb, ib) = out
-    assert ia["recoveries"] > 0 and ia["launches"] > ia["recoveries"], ia
+    assert ia["recoveries"] > 0 and ia["launches"] >= ia["recoveries"], ia
     assert np.array_equal(pa, pb) and np.array_equal(ka, kb) and ra == rb
     for k in ("pos", "vel", "force", "ids"):
         assert np.array_equal(sa[k], sb[k]), k
