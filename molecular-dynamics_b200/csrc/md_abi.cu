@@ -773,7 +773,8 @@ md_status kick_drift_async(md_system* s, md_nlist* nl, double dt, bool check_ski
 // rebuilt. Afterwards the float frames match the positions whenever the list uses tiles.
 md_status drift_and_update(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, bool* rebuilt) {
     const bool current = nlist_current(nl, s);
-    const bool frames = current && nl->use_tiles && (ff->precision == MD_PREC_FP32FX || ff->precision == MD_PREC_FP32);
+    const bool frames = current && nl->use_tiles &&
+                        (ff->precision == MD_PREC_FP32FX || ff->precision == MD_PREC_FP32 || ff->precision == MD_PREC_FX32);
     MD_TRY(kick_drift_async(s, nl, dt, current, frames));
     bool stale = true;
     if (current) {

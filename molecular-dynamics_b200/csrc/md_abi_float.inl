@@ -146,7 +146,9 @@ md_status forces_list_fx64_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
 // MD_PREC_FX32 evaluates pairs closer than this many sigma (plus the skin, at the list build) in double
 constexpr double kFx32NearSigma = 1.3;
 
-// MD_PREC_FX32's near-first rows of the list's last build (k_rows_near_first), made once per build and near radius
+// MD_PREC_FX32's near-first rows of the list's last build (k_rows_near_first), made once per build and near
+// radius. The classification reads the float frames of the list's reference positions, made here into the spare
+// frame buffer (free between steps; a fused force kernel writes it only after this).
 md_status ensure_near_first(md_forcefield* ff, md_system* s, md_nlist* nl) {
     const int n = static_cast<int>(s->n);
     const double near = kFx32NearSigma * ff->sigma + nl->skin;
@@ -154,8 +156,19 @@ md_status ensure_near_first(md_forcefield* ff, md_system* s, md_nlist* nl) {
     if (n == 0 || (nl->nf_build == nl->builds && nl->nf_near2 == near2)) return MD_OK;
     MD_CUDA(nl->rows_nf.reserve(row_buffer_entries(n, nl->cap)));
     MD_CUDA(nl->counts_nf.reserve(n));
-    k_rows_near_first<<<blocks_for(n, 128), 128, 0, s->stream>>>(nl->ref_pos.p, n, s->box, near2, nl->rows.p, nl->cap,
-                                                                 nl->counts.p, nl->rows_nf.p, nl->counts_nf.p);
+    MD_CUDA(nl->frames2.reserve(static_cast<size_t>(n) + 1));
+    k_frames<<<blocks_for(n + 1, kThreads), kThreads, 0, s->stream>>>(nl->ref_pos.p, n, nl->cell_sorted.p,
+                                                                      nl->grid.ncps, cell_side(nl, s), s->box,
+                                                                      nl->frames2.p);
+    MD_CHECK_LAUNCH();
+    // a block of up to 4 warps, each staging its 32 rows of cap + 1 entries in shared memory (at most 100 KB)
+    const size_t row_bytes = 32 * (static_cast<size_t>(nl->cap) + 1) * sizeof(uint32_t);
+    const int warps = static_cast<int>(std::clamp<size_t>(100 * 1024 / row_bytes, 1, 4));
+    const size_t smem = warps * row_bytes;
+    MD_CUDA(allow_smem(k_rows_near_first, smem));
+    k_rows_near_first<<<blocks_for(n, 32 * warps), 32 * warps, smem, s->stream>>>(
+        nl->frames2.p, n, cell_offsets(nl, s), static_cast<float>(near2), nl->rows.p, nl->cap, nl->counts.p,
+        nl->rows_nf.p, nl->counts_nf.p);
     MD_CHECK_LAUNCH();
     nl->nf_build = nl->builds;
     nl->nf_near2 = near2;
@@ -167,25 +180,19 @@ md_status ensure_near_first(md_forcefield* ff, md_system* s, md_nlist* nl) {
 // kinetic energy and optionally the next drift fused as in forces_list_fx64_async. Boxes under 3 cells per side
 // take the MD_PREC_FX64 small-box kernel (every pair in double).
 md_status forces_list_fx32_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool want_energy, double kick_dt,
-                                 bool* fused_ke, bool fixed_fresh, bool fuse_drift) {
+                                 bool* fused_ke, bool frames_fresh, bool fixed_fresh, bool fuse_drift) {
     if (!nl->use_cells) return forces_list_fx64_async(ff, s, nl, want_energy, kick_dt, fused_ke, fixed_fresh, fuse_drift);
     const int n = static_cast<int>(s->n);
     const bool kick = kick_dt > 0.0;
     const Fx64LJ dlj = fx64_lj(ff);
-    // the float path works in frame units (2^-28): sigma^2, r_c^2 and the band scaled by 2^56. The float r^2 of
-    // an exact separation rounded once per component is within ~6e-7 of r^2 (relative): a shell of 1e-5 r_c^2
-    // holds every pair whose float and exact cutoff tests could disagree
-    FloatLJ flj = float_lj(ff);
-    constexpr double kFrameArea = kFrameScale * kFrameScale;  // 2^56
-    flj.sig2 = static_cast<float>(ff->lj.sig2 * kFrameArea);
-    flj.rc2 = static_cast<float>(ff->lj.rc2 * kFrameArea);
-    flj.band = static_cast<float>(1e-5 * ff->lj.rc2 * kFrameArea);
+    const FloatLJ flj = float_lj(ff);
     MD_CUDA(ff->fx_acc.reserve(4));
     if (want_energy || kick) MD_CUDA(cudaMemsetAsync(ff->fx_acc.p, 0, 4 * sizeof(long long), s->stream));
     auto* acc = reinterpret_cast<unsigned long long*>(ff->fx_acc.p);
     nl->variant[MD_PREC_FX32] = 0;
     if (n > 0) {
         MD_TRY(ensure_near_first(ff, s, nl));
+        if (!frames_fresh) MD_TRY(frames_async(s, nl));
         MD_CUDA(nl->iframes.reserve(n));
         if (!fixed_fresh) {
             k_frames_fixed<<<blocks_for(n, kThreads), kThreads, 0, s->stream>>>(s->pos.p, n, nl->cell_sorted.p,
@@ -195,13 +202,15 @@ md_status forces_list_fx32_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
         }
         KickArgs ka{kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
         const bool fuse = fuse_drift && kick;
-        if (fuse) {  // the next step's kick and drift, new positions and fixed-point frames to spare buffers
+        if (fuse) {  // the next step's kick and drift, new positions and both kinds of frames to spare buffers
             MD_CUDA(s->pos2.reserve(n));
             MD_CUDA(nl->iframes2.reserve(n));
+            MD_CUDA(nl->frames2.reserve(static_cast<size_t>(n) + 1));
             MD_CUDA(cudaMemsetAsync(nl->flags.p, 0, sizeof(int), s->stream));
             ka.pos_in = s->pos.p;
             ka.pos_out = s->pos2.p;
             ka.iframes_out = nl->iframes2.p;
+            ka.frames_out = nl->frames2.p;
             ka.ref_pos = nl->ref_pos.p;
             ka.max_disp2 = nl->max_disp2;
             ka.stale = nl->flags.p;
@@ -212,6 +221,7 @@ md_status forces_list_fx32_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
             ka.box = s->box;
         }
         const FixedOffsets offs = fixed_offsets(nl, s);
+        const CellOffsets foffs = cell_offsets(nl, s);
         auto go = [&](auto kernel, unsigned& grid) -> md_status {
             if (grid == 0) {
                 int sms = 0, per_sm = 0;
@@ -221,8 +231,8 @@ md_status forces_list_fx32_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
             }
             MD_TRY(profile_mark(s));
             kernel<<<std::min(blocks_for(n, 128), grid), 128, 0, s->stream>>>(
-                nl->iframes.p, s->pos.p, n, s->box, dlj, flj, offs, nl->rows_nf.p, nl->cap, nl->counts_nf.p,
-                s->force.p, acc, ka);
+                nl->iframes.p, nl->frames.p, s->pos.p, n, s->box, dlj, flj, offs, foffs, nl->rows_nf.p, nl->cap,
+                nl->counts_nf.p, s->force.p, acc, ka);
             MD_CHECK_LAUNCH();
             return profile_mark(s);
         };
@@ -233,6 +243,7 @@ md_status forces_list_fx32_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
         if (fuse) {
             swap_buffers(s->pos, s->pos2);
             swap_buffers(nl->iframes, nl->iframes2);
+            swap_buffers(nl->frames, nl->frames2);
         }
     }
     const bool ke_fused = kick && n > 0;
@@ -252,7 +263,7 @@ md_status forces_list_float_async(md_forcefield* ff, md_system* s, md_nlist* nl,
     if (ff->precision == MD_PREC_FX64)
         return forces_list_fx64_async(ff, s, nl, want_energy, kick_dt, fused_ke, fixed_fresh, fuse_drift);
     if (ff->precision == MD_PREC_FX32)
-        return forces_list_fx32_async(ff, s, nl, want_energy, kick_dt, fused_ke, fixed_fresh, fuse_drift);
+        return forces_list_fx32_async(ff, s, nl, want_energy, kick_dt, fused_ke, frames_fresh, fixed_fresh, fuse_drift);
     const int n = static_cast<int>(s->n);
     const bool fixed = ff->precision == MD_PREC_FP32FX;
     const bool kick = kick_dt > 0.0;

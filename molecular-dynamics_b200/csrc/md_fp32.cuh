@@ -214,16 +214,14 @@ struct FloatAcc {
             w_fx += __float2ll_rn(gw * kEnergyScale);
         }
     }
-    // A float group of MD_PREC_FX32 (whose rows hold float and double groups): its force summed in frame units
-    // (2^-28 of a force unit, so 2^60 fixed-point units each) and its energy and virial in the finer 2^-30 units of
-    // the double groups (the products with powers of two are exact)
-    __device__ __forceinline__ void add_group_frame(float gx, float gy, float gz, float ge, float gw, long long& e_fx,
-                                                    long long& w_fx) {
-        static_assert(kFixed, "frame-unit groups accumulate in fixed point");
-        constexpr float kFrameForceScale = 1152921504606846976.0f;  // 2^60
-        ax += __float2ll_rn(gx * kFrameForceScale);
-        ay += __float2ll_rn(gy * kFrameForceScale);
-        az += __float2ll_rn(gz * kFrameForceScale);
+    // A float group whose energy and virial go into the finer 2^-30 units of the double groups (MD_PREC_FX32,
+    // whose rows hold both kinds); forces in the same 2^-32 units (the products with 2^32 and 2^30 are exact)
+    __device__ __forceinline__ void add_group_fine(float gx, float gy, float gz, float ge, float gw, long long& e_fx,
+                                                   long long& w_fx) {
+        static_assert(kFixed, "fine groups accumulate in fixed point");
+        ax += __float2ll_rn(gx * kForceScale);
+        ay += __float2ll_rn(gy * kForceScale);
+        az += __float2ll_rn(gz * kForceScale);
         if (kEnergy) {
             e_fx += __float2ll_rn(ge * static_cast<float>(kEnergyScale64));
             w_fx += __float2ll_rn(gw * static_cast<float>(kEnergyScale64));

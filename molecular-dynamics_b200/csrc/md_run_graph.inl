@@ -188,9 +188,12 @@ md_status device_rebuild_async(md_system* s, md_forcefield* ff, md_nlist* nl, co
     MD_CHECK_LAUNCH();
     k_build_done<<<1, 1, 0, st>>>(nl->flags.p + 1, nl->cap, s->graph_state.p, (s->graph_flags & MD_GRAPH_TEST_RERUN) != 0);
     MD_CHECK_LAUNCH();
-    if (ff->precision == MD_PREC_FX32) {
-        k_rows_near_first<<<blocks_for(n, 128), 128, 0, st>>>(nl->ref_pos.p, n, s->box, nl->nf_near2, nl->rows.p,
-                                                              nl->cap, nl->counts.p, nl->rows_nf.p, nl->counts_nf.p);
+    if (ff->precision == MD_PREC_FX32) {  // the rows just built, near-first (the float frames are the build's)
+        const size_t row_bytes = 32 * (static_cast<size_t>(nl->cap) + 1) * sizeof(uint32_t);
+        const int warps = static_cast<int>(std::clamp<size_t>(100 * 1024 / row_bytes, 1, 4));
+        k_rows_near_first<<<blocks_for(n, 32 * warps), 32 * warps, warps * row_bytes, st>>>(
+            nl->frames.p, n, cell_offsets(nl, s), static_cast<float>(nl->nf_near2), nl->rows.p, nl->cap, nl->counts.p,
+            nl->rows_nf.p, nl->counts_nf.p);
         MD_CHECK_LAUNCH();
     }
     if (ff->precision == MD_PREC_FX64 || ff->precision == MD_PREC_FX32) {
@@ -261,7 +264,8 @@ std::string graph_key(const md_system* s, const md_forcefield* ff, const md_nlis
 md_status graph_step(md_system* s, md_forcefield* ff, md_nlist* nl, const md_run_options& o, const RunStep& r, int k,
                      double dt, bool want_energy, bool want_ke, double bussi_c, cudaGraph_t graph, const TileGeom& tg,
                      uint64_t* body_kernels) {
-    const bool float_frames = ff->precision == MD_PREC_FP32FX || ff->precision == MD_PREC_FP32;
+    const bool float_frames =
+        ff->precision == MD_PREC_FP32FX || ff->precision == MD_PREC_FP32 || ff->precision == MD_PREC_FX32;
     if (!r.drifted_in) MD_TRY(kick_drift_async(s, nl, dt, true, float_frames));
     cudaGraphConditionalHandle h;
     MD_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault));
@@ -343,6 +347,10 @@ md_status chunk_graph(md_system* s, md_forcefield* ff, md_nlist* nl, const md_ru
     // profiling events (two per step)
     const size_t build_smem = sizeof(float4) * tg.max_staged, tile_smem = sizeof(float4) * (tg.max_staged + 1);
     MD_CUDA(allow_smem(k_nlist_build_tile, build_smem));
+    {
+        const size_t row_bytes = 32 * (static_cast<size_t>(nl->cap) + 1) * sizeof(uint32_t);
+        MD_CUDA(allow_smem(k_rows_near_first, std::clamp<size_t>(100 * 1024 / row_bytes, 1, 4) * row_bytes));
+    }
     MD_CUDA(allow_smem(k_force_fp32_tile<true, true>, tile_smem));
     MD_CUDA(allow_smem(k_force_fp32_tile<true, false>, tile_smem));
     MD_CUDA(allow_smem(k_force_fp32_tile<false, true>, tile_smem));
