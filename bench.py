@@ -79,6 +79,9 @@ def args_parse():
                    help="trajectory length of the differentiation workload (N = 32,000; 0: skip)")
     p.add_argument("--force-variant", type=int, default=-1,
                    help="list force kernel of the headline run: -1 autotunes, 0-4 pin one (md_nlist_set_force_variant)")
+    p.add_argument("--graph-chunk", type=int, default=64,
+                   help="md_run's CUDA-graph chunk length (md_system_set_graph); 0 runs every step from the host, as "
+                        "profilers need (ncu cannot profile kernels in graphs with conditional nodes)")
     p.add_argument("--profile-region", action="store_true",
                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return p.parse_args()
@@ -426,6 +429,7 @@ def run_gpu_arm(a):
     n = 4 * a.cells ** 3
     dt = 0.005
     s = md.fcc_system(a.cells, a.density, a.temperature, seed=42 + rank, device=local)
+    s.set_graph(a.graph_chunk)
     nl = md.NeighbourList(2.5, 0.3)
     if a.force_variant >= 0:
         nl.set_force_variant(prec, a.force_variant)

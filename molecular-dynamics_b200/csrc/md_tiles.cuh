@@ -217,10 +217,6 @@ __device__ __forceinline__ void scan_cell(const float4* q, int jbase, int u0, in
     const float2 nxy = make_float2(-qo.x, -qo.y);
     const float nz = -qo.z;
     if (cnt + (u1 - u0) <= cap) {  // every candidate fits: no capacity test per candidate
-#ifdef MD_SCAN_UNROLL
-        constexpr int kScanUnroll = MD_SCAN_UNROLL;
-#pragma unroll kScanUnroll
-#endif
         for (int u = u0; u < u1; ++u) {
             const float4 qj = q[u];
             const float2 d = __fadd2_rn(make_float2(qj.x, qj.y), nxy);
