@@ -144,7 +144,7 @@ md_status forces_list_fx64_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
 }
 
 // MD_PREC_FX32 evaluates pairs closer than this many sigma (plus the skin, at the list build) in double
-constexpr double kFx32NearSigma = 1.3;
+constexpr double kFx32NearSigma = 1.2;
 
 // MD_PREC_FX32's near-first rows of the list's last build (k_rows_near_first), made once per build and near
 // radius. The classification reads the float frames of the list's reference positions, made here into the spare

@@ -3,10 +3,10 @@
 //
 // Why the split: a float pair term carries a relative error of a few 1e-7 (the force goes as r^-14, so the
 // rounding of r^2 alone is amplified sevenfold). That is below 1e-6 of a particle's net force only where the
-// pair force itself is small. Pairs beyond about 1.3 sigma have |F| <= 2.3 eps/sigma; the few closer pairs (about
-// one in six of a row) carry forces up to 1e2 and, evaluated in float, leave 60 % of particles above 1e-6
-// relative error. So every row is reordered once per list build: entries whose pair was closer than
-// (near_sigma sigma + skin) at the build come first and are evaluated in double on the 32-bit fixed-point frames
+// pair force itself is small. Pairs beyond 1.2 sigma have |F| <= 2.4 eps/sigma; the few closer pairs (about one in
+// six of a row) carry forces up to 1e2 and, evaluated in float, leave 60 % of particles above 1e-6 relative
+// error. So every row is reordered once per list build: entries whose pair was closer than (1.2 sigma + skin)
+// at the build come first, and its first two groups of 8 are evaluated in double on the 32-bit fixed-point frames
 // (2^-28 units) of MD_PREC_FX64, whose integer differences are exact separations; the rest are evaluated in float
 // on the float frames of MD_PREC_FP32FX, with its pinned operation sequence. Between rebuilds every particle
 // stays within skin/2 of its build position, so a pair evaluated in float is never closer than near_sigma sigma.
@@ -21,9 +21,15 @@
 
 namespace md {
 
+constexpr int kFx32NearGroups = 2;  // row groups of 8 entries evaluated in double
+
 // Near-first rows. For particle i: the entries of its row whose pair was closer than sqrt(near2) at the list
 // build, in their row order, then sentinel entries up to the next multiple of 8 that the remaining entries do not
-// fill, then the remaining entries in reverse row order; counts_nf[i] = (groups holding a near entry, all groups).
+// fill, then the remaining entries in reverse row order; counts_nf[i] = (the first kFx32NearGroups groups, or all
+// of a shorter row; all groups). Every row gets the same number of double groups, so the warps of the force kernel
+// never split between the two paths; a row with more than 8 kFx32NearGroups near entries keeps the closest ones
+// there and moves the farthest to the float groups (rare: about 12 pairs lie closer than 1.5 sigma at liquid
+// density, and those moved are the farthest of them).
 // The classification uses ref_frames, the float frames of the list's reference positions (the positions of the
 // build), with the float offsets of the entries' cell codes. Rows keep the interleaved layout and capacity of the
 // list's rows. A warp builds the rows of its 32 particles in shared memory (stride cap + 1 entries, so the lanes'
@@ -60,9 +66,27 @@ __global__ void k_rows_near_first(const float4* __restrict__ ref_frames, int n, 
                     my[--back] = e;
             }
         }
+        // more near entries than the double groups hold: move the farthest to the float part, one at a time
+        while (front > 8 * kFx32NearGroups) {
+            int far_k = 0;
+            float far_r2 = -1.0f;
+            for (int k = 0; k < front; ++k) {
+                const uint32_t e = my[k];
+                float dx, dy, dz;
+                const float r2 = float_separation(qi, ref_frames[e & kIndexMask], s_off[e >> kCodeShift], dx, dy, dz);
+                if (r2 > far_r2) {
+                    far_r2 = r2;
+                    far_k = k;
+                }
+            }
+            const uint32_t e = my[far_k];
+            my[far_k] = my[--front];
+            my[--back] = e;
+        }
         const uint32_t pad = static_cast<uint32_t>(n) | (kSentinelCode << kCodeShift);
         for (int s = front; s < back; ++s) my[s] = pad;
-        counts_nf[i] = make_int2((front + 7) >> 3, ((m + 7) & ~7) >> 3);
+        const int groups = ((m + 7) & ~7) >> 3;
+        counts_nf[i] = make_int2(groups < kFx32NearGroups ? groups : kFx32NearGroups, groups);
     }
     __syncwarp();
     const int quads = ((m + 7) & ~7) >> 2;
