@@ -75,6 +75,9 @@ def args_parse():
     p.add_argument("--replica-steps", type=int, default=5000,
                    help="steps of the batched-replica workload (512 replicas; 0: skip)")
     p.add_argument("--replicas", type=int, default=512)
+    p.add_argument("--replica-precision", choices=["fp64", "fp32fx", "fp32"], default=None,
+                   help="precision of the batched-replica workload (default: the headline precision where the batch "
+                        "engine has it, else fp32fx)")
     p.add_argument("--adjoint-steps", type=int, default=200,
                    help="trajectory length of the differentiation workload (N = 32,000; 0: skip)")
     p.add_argument("--force-variant", type=int, default=-1,
@@ -324,8 +327,8 @@ def replica_workload(md, a, device: int) -> dict:
         d = s.download()
         systems.append((d["pos"], s.box, d["vel"], None))
         del s
-    prec = PRECISIONS[a.precision][0]
-    b = md.Batch(systems, precision=prec, thermostat="bussi", temperatures=temp, seeds=1000 + np.arange(R),
+    name = a.replica_precision or (a.precision if a.precision in ("fp64", "fp32fx", "fp32") else "fp32fx")
+    b = md.Batch(systems, precision=PRECISIONS[name][0], thermostat="bussi", temperatures=temp, seeds=1000 + np.arange(R),
                  bussi_tau=0.1, energy_every=10, chunk_steps=100, device=device)
     info = b.info()
     b.run(100)
@@ -347,7 +350,7 @@ def replica_workload(md, a, device: int) -> dict:
     return {"workload": f"{R} replicas, n~U[4,20] (N 256-32000), rho~U[0.7,0.95], T~U[0.7,2.0], Bussi tau=0.1, "
                         f"dt=0.005, rc=2.5, skin=0.3, {a.replica_steps} steps",
             "atoms": info["atoms"], "value": info["atoms"] * a.replica_steps / (ms / 1e3), "unit": "atom-steps/s",
-            "ms_per_step": ms / a.replica_steps, "precision": a.precision,
+            "ms_per_step": ms / a.replica_steps, "precision": name,
             "force_variant": b.force_variant(), "gpu_launches": b.info()["launches"] - l0,
             "rebuilds_per_replica_mean": float(b.rebuilds().mean()),
             "pe_per_atom_stderr": {"median": float(np.median(pe_err)), "max": float(pe_err.max())},

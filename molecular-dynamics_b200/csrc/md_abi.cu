@@ -233,7 +233,7 @@ struct md_nlist {
     int variant[5] = {-1, -1, -1, -1, -1};  // force kernel per precision (0 global gathers, 1 tile; -1 untuned)
     int pinned[5] = {-1, -1, -1, -1, -1};   // set by md_nlist_set_force_variant
     uint64_t builds = 0;                    // list builds so far (names the rows of the last one)
-    // MD_PREC_FX32's near-first copy of the rows (k_rows_near_first) and its (near groups, groups) counts, for
+    // MD_PREC_FX32's near rows and then far rows (k_rows_split) and their (near groups, far groups) counts, for
     // build nf_build with the near radius^2 nf_near2
     DevBuf<uint32_t> rows_nf;
     DevBuf<int2> counts_nf;

@@ -146,36 +146,48 @@ md_status forces_list_fx64_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
 // MD_PREC_FX32 evaluates pairs closer than this many sigma (plus the skin, at the list build) in double
 constexpr double kFx32NearSigma = 1.2;
 
-// MD_PREC_FX32's near-first rows of the list's last build (k_rows_near_first), made once per build and near
-// radius. The classification reads the float frames of the list's reference positions, made here into the spare
-// frame buffer (free between steps; a fused force kernel writes it only after this).
+// MD_PREC_FX32's near and far rows of the rows just built, classified on ref_frames (the float frames of the
+// build's positions): k_rows_split, then k_rows_split_fix for the rows with more near entries than a near row
+// holds. rows_nf holds the near rows and, after them, the far rows.
+md_status split_rows_async(md_system* s, md_nlist* nl, const float4* ref_frames, float near2, cudaStream_t st) {
+    const int n = static_cast<int>(s->n);
+    uint32_t* near_rows = nl->rows_nf.p;
+    uint32_t* far_rows = nl->rows_nf.p + fx32_near_entries(n);
+    k_rows_split<<<blocks_for(n, kSplitThreads), kSplitThreads, 0, st>>>(
+        ref_frames, n, cell_offsets(nl, s), near2, nl->rows.p, nl->cap, nl->counts.p, near_rows, far_rows,
+        nl->counts_nf.p);
+    MD_CHECK_LAUNCH();
+    k_rows_split_fix<<<std::min(blocks_for(n, 128), 1184u), 128, 0, st>>>(ref_frames, n, cell_offsets(nl, s), near2,
+                                                                         nl->rows.p, nl->cap, nl->counts.p, near_rows,
+                                                                         far_rows, nl->counts_nf.p);
+    MD_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+// MD_PREC_FX32's near and far rows of the list's last build, made once per build and near radius. The
+// classification reads the float frames of the list's reference positions, made here into the spare frame buffer
+// (free between steps; a fused force kernel writes it only after this).
 md_status ensure_near_first(md_forcefield* ff, md_system* s, md_nlist* nl) {
     const int n = static_cast<int>(s->n);
     const double near = kFx32NearSigma * ff->sigma + nl->skin;
     const double near2 = near * near;
     if (n == 0 || (nl->nf_build == nl->builds && nl->nf_near2 == near2)) return MD_OK;
-    MD_CUDA(nl->rows_nf.reserve(row_buffer_entries(n, nl->cap)));
+    const size_t entries = fx32_near_entries(n) + row_buffer_entries(n, nl->cap);
+    if (entries / 4 > 0xffffffffull) return fail(MD_ERR_INVALID, "MD_PREC_FX32: the split rows exceed 2^32 quads");
+    MD_CUDA(nl->rows_nf.reserve(entries));
     MD_CUDA(nl->counts_nf.reserve(n));
     MD_CUDA(nl->frames2.reserve(static_cast<size_t>(n) + 1));
     k_frames<<<blocks_for(n + 1, kThreads), kThreads, 0, s->stream>>>(nl->ref_pos.p, n, nl->cell_sorted.p,
                                                                       nl->grid.ncps, cell_side(nl, s), s->box,
                                                                       nl->frames2.p);
     MD_CHECK_LAUNCH();
-    // a block of up to 4 warps, each staging its 32 rows of cap + 1 entries in shared memory (at most 100 KB)
-    const size_t row_bytes = 32 * (static_cast<size_t>(nl->cap) + 1) * sizeof(uint32_t);
-    const int warps = static_cast<int>(std::clamp<size_t>(100 * 1024 / row_bytes, 1, 4));
-    const size_t smem = warps * row_bytes;
-    MD_CUDA(allow_smem(k_rows_near_first, smem));
-    k_rows_near_first<<<blocks_for(n, 32 * warps), 32 * warps, smem, s->stream>>>(
-        nl->frames2.p, n, cell_offsets(nl, s), static_cast<float>(near2), nl->rows.p, nl->cap, nl->counts.p,
-        nl->rows_nf.p, nl->counts_nf.p);
-    MD_CHECK_LAUNCH();
+    MD_TRY(split_rows_async(s, nl, nl->frames2.p, static_cast<float>(near2), s->stream));
     nl->nf_build = nl->builds;
     nl->nf_near2 = near2;
     return MD_OK;
 }
 
-// MD_PREC_FX32 list forces: after each list build the rows are reordered near-first (k_rows_near_first, once per
+// MD_PREC_FX32 list forces: after each list build the rows are split into near and far rows (once per
 // build and near radius); then the fixed-point frames and k_force_fx32 on a resident grid, with the closing kick,
 // kinetic energy and optionally the next drift fused as in forces_list_fx64_async. Boxes under 3 cells per side
 // take the MD_PREC_FX64 small-box kernel (every pair in double).
@@ -231,7 +243,8 @@ md_status forces_list_fx32_async(md_forcefield* ff, md_system* s, md_nlist* nl, 
             }
             MD_TRY(profile_mark(s));
             kernel<<<std::min(blocks_for(n, 128), grid), 128, 0, s->stream>>>(
-                nl->iframes.p, nl->frames.p, s->pos.p, n, s->box, dlj, flj, offs, foffs, nl->rows_nf.p, nl->cap,
+                nl->iframes.p, nl->frames.p, s->pos.p, n, s->box, dlj, flj, offs, foffs,
+                reinterpret_cast<const uint4*>(nl->rows_nf.p), static_cast<unsigned>(fx32_near_entries(n) / 4), nl->cap,
                 nl->counts_nf.p, s->force.p, acc, ka);
             MD_CHECK_LAUNCH();
             return profile_mark(s);

@@ -188,14 +188,8 @@ md_status device_rebuild_async(md_system* s, md_forcefield* ff, md_nlist* nl, co
     MD_CHECK_LAUNCH();
     k_build_done<<<1, 1, 0, st>>>(nl->flags.p + 1, nl->cap, s->graph_state.p, (s->graph_flags & MD_GRAPH_TEST_RERUN) != 0);
     MD_CHECK_LAUNCH();
-    if (ff->precision == MD_PREC_FX32) {  // the rows just built, near-first (the float frames are the build's)
-        const size_t row_bytes = 32 * (static_cast<size_t>(nl->cap) + 1) * sizeof(uint32_t);
-        const int warps = static_cast<int>(std::clamp<size_t>(100 * 1024 / row_bytes, 1, 4));
-        k_rows_near_first<<<blocks_for(n, 32 * warps), 32 * warps, warps * row_bytes, st>>>(
-            nl->frames.p, n, cell_offsets(nl, s), static_cast<float>(nl->nf_near2), nl->rows.p, nl->cap, nl->counts.p,
-            nl->rows_nf.p, nl->counts_nf.p);
-        MD_CHECK_LAUNCH();
-    }
+    if (ff->precision == MD_PREC_FX32)  // the rows just built, split (the float frames are the build's)
+        MD_TRY(split_rows_async(s, nl, nl->frames.p, static_cast<float>(nl->nf_near2), st));
     if (ff->precision == MD_PREC_FX64 || ff->precision == MD_PREC_FX32) {
         k_frames_fixed<<<blocks_for(n, kThreads), kThreads, 0, st>>>(s->pos.p, n, nl->cell_sorted.p, g.ncps, cell,
                                                                      s->box, nl->iframes.p);
@@ -347,10 +341,6 @@ md_status chunk_graph(md_system* s, md_forcefield* ff, md_nlist* nl, const md_ru
     // profiling events (two per step)
     const size_t build_smem = sizeof(float4) * tg.max_staged, tile_smem = sizeof(float4) * (tg.max_staged + 1);
     MD_CUDA(allow_smem(k_nlist_build_tile, build_smem));
-    {
-        const size_t row_bytes = 32 * (static_cast<size_t>(nl->cap) + 1) * sizeof(uint32_t);
-        MD_CUDA(allow_smem(k_rows_near_first, std::clamp<size_t>(100 * 1024 / row_bytes, 1, 4) * row_bytes));
-    }
     MD_CUDA(allow_smem(k_force_fp32_tile<true, true>, tile_smem));
     MD_CUDA(allow_smem(k_force_fp32_tile<true, false>, tile_smem));
     MD_CUDA(allow_smem(k_force_fp32_tile<false, true>, tile_smem));

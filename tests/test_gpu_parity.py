@@ -235,13 +235,15 @@ def test_total_force_and_momentum(md, golden):
 
 
 @pytest.mark.parametrize("prec", ["PREC_FX64", "PREC_FX32"])
-@pytest.mark.parametrize("cells,density", [(8, 0.8442), (6, 0.5), (20, 1.0)])
+@pytest.mark.parametrize("cells,density", [(8, 0.8442), (6, 0.5), (20, 1.0), (10, 1.3)])
 def test_fixed_point_modes_per_particle_force_error(md, golden, cells, density, prec):
     """MD_PREC_FX64 (exact fixed-point separations, double pair terms) and MD_PREC_FX32 (the same separations,
     float pair terms except for the close pairs, which are double): every particle's force within 1e-6 of the rms
     force of the FP64 path, 99 % of particles within 1e-6 of their own force, PE and virial close to FP64's
     (FX64 within 5e-8 relative; FX32 within 1e-6 and 1e-5: its float pair energies round at ~6e-8 each), the same
-    inside count, bit-identical repeats. Melted liquid states (config 1's after 1000 steps, and melted boxes)."""
+    inside count, bit-identical repeats. Melted liquid states (config 1's after 1000 steps, and melted boxes), and a
+    compressed solid (rho = 1.3: 18 neighbours within 1.5 sigma, so FX32's rows hold more close entries than its
+    double groups and take the closest 16)."""
     if cells == 8:
         s, nl = liquid(md, golden)
     else:
