@@ -41,9 +41,9 @@ typedef enum md_precision {
     MD_PREC_FP32 = 2,   /* float pair arithmetic, float accumulation */
     MD_PREC_FX64 = 3,   /* exact separations from 32-bit fixed-point frames, double pair terms, 64-bit
                            fixed-point accumulation */
-    MD_PREC_FX32 = 4    /* double pair terms on exact separations (32-bit fixed-point frames) for the 16 row
-                           entries first in a per-build ordering that puts the pairs closer than 1.2 sigma + skin
-                           first; float pair terms (MD_PREC_FP32FX's) for the rest; 64-bit fixed-point sums */
+    MD_PREC_FX32 = 4    /* double pair terms on exact separations (32-bit fixed-point frames) for the pairs
+                           closer than 1.2 sigma + skin at the list build (at most the 16 closest of a row), float
+                           pair terms (MD_PREC_FP32FX's) for the rest; 64-bit fixed-point sums */
 } md_precision;
 
 typedef struct md_system md_system;         /* System (include/System.hpp:12) */
