@@ -6,9 +6,11 @@ neighbour list at its natural rebuild rate, LJ forces, integration) on the 4,000
 
 Workload (the large single system of the benchmark): FCC 100^3 x 4 = 4,000,000 atoms, density 0.8442,
 T* = 0.71 after a 200-step rescale equilibration from a T = 2 melt (md_sim's --melt schedule), r_c = 2.5
-truncated and shifted, skin 0.3, dt 0.005, NVE. The headline precision is FP32 pair arithmetic with 64-bit
-fixed-point force accumulation; the FP64 path (bit-identical to the reference's deterministic mode) is timed
-beside it on the same state. Inputs are synthetic (seeded lattice and velocities) and the working set
+truncated and shifted, skin 0.3, dt 0.005, NVE. The headline precision is MD_PREC_FX32 (FP32 pair arithmetic
+with 64-bit fixed-point force accumulation, the close pairs in double on exact fixed-point separations), the
+mode that keeps every particle's force within 1e-6 of the FP64 path; the FP64 path (bit-identical to the
+reference's deterministic mode) is timed beside it on the same state, and FP32FX (float for every pair) and
+the other modes beside that. Inputs are synthetic (seeded lattice and velocities) and the working set
 (~1.4 GB) is far larger than the 126 MB L2.
 
 One rank per GPU (torchrun); ranks run independent replicas (seed 42 + rank), so scaling is weak and no
@@ -53,7 +55,7 @@ def args_parse():
     p.add_argument("--density", type=float, default=0.8442)
     p.add_argument("--temperature", type=float, default=0.71)
     p.add_argument("--equil", type=int, default=200)
-    p.add_argument("--precision", choices=list(PRECISIONS), default="fp32fx")
+    p.add_argument("--precision", choices=list(PRECISIONS), default="fx32")
     p.add_argument("--fp64-steps", type=int, default=None,
                    help="steps of the FP64 comparison run from the headline's starting state (default: --steps; 0: skip)")
     p.add_argument("--side-steps", type=int, default=300,
@@ -258,10 +260,10 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
 
 
-def ncu_traffic_per_atom():
-    """DRAM bytes per atom of the force kernel from the committed ncu summary, or None."""
+def ncu_traffic_per_atom(precision: str):
+    """DRAM bytes per atom of the precision's force kernel from the committed ncu summary, or None."""
     try:
-        with open(os.path.join(ROOT, "profiles", "force_fp32fx_traffic.json")) as f:
+        with open(os.path.join(ROOT, "profiles", f"force_{precision}_traffic.json")) as f:
             d = json.load(f)
         return float(d["dram_bytes_per_launch"]) / float(d["n_atoms"])
     except (OSError, KeyError, ValueError):
@@ -585,7 +587,9 @@ def run_gpu_arm(a):
     if a.precision == "fp64":
         bytes_per_atom += 16 * pairs / n
     achieved = bytes_per_atom * n / kernel_s / 1e9
-    tpa = ncu_traffic_per_atom() if a.precision == "fp32fx" else None
+    if a.precision == "fx32":
+        bytes_per_atom += 32  # the own fixed-point frame read and the next one written, beside the float frames
+    tpa = ncu_traffic_per_atom(a.precision)
     # the FP32-pipe side of the roofline (the force kernel sits between the two): 23 flop per ordered pair of
     # the full list (separation, r^2, reciprocal, F/r, three accumulating FMAs) and 6 per unordered pair for the
     # energy and virial, against the nominal FP32 peak (SMs x 128 lanes x 2 flop x the max SM clock sampled)
