@@ -253,15 +253,19 @@ struct md_forcefield {
     bool deterministic = false;
     double virial = 0.0, inside = 0.0;
     int device = -1;
-    DevBuf<double2> eblocks;
-    // FP64 energies: (pairEnergy, pairVirial) of every own pair, in pair order, in two buffers used in turn: the
-    // ordered sums of one step run on a second stream (side) while the next step's force kernel fills the other
-    DevBuf<double2> pair_ew[2];
-    int ew_next = 0;
-    cudaStream_t side = nullptr;
-    cudaEvent_t ev_force = nullptr, ev_done = nullptr, ev_read[2] = {nullptr, nullptr};
-    bool read_pending[2] = {false, false};  // ev_read[b] marks the last sums that read pair_ew[b]
-    bool side_pending = false;              // ev_done marks side-stream sums the system's stream has not joined
+    // FP64 energies: r^2 of every own pair, in pair order, in two buffers used in turn. The ordered sums of one
+    // step run on two more streams while the next step's force kernel fills the other buffer: the 1024-pair block
+    // sums on `side`, the chain over the block sums (one warp) on `chain`, with the block sums in two buffers too,
+    // so that the next step's block sums never wait for this step's chain. Both streams have the device's highest
+    // priority, so that their blocks are not queued behind the next step's force kernel.
+    DevBuf<double> pair_r2[2];
+    DevBuf<double2> eblocks[2];
+    int ew_next = 0, eb_next = 0;
+    cudaStream_t side = nullptr, chain = nullptr;
+    cudaEvent_t ev_force = nullptr, ev_done = nullptr, ev_read[2] = {nullptr, nullptr}, ev_chain[2] = {nullptr, nullptr};
+    bool read_pending[2] = {false, false};   // ev_read[b] marks the last block sums that read pair_r2[b]
+    bool chain_pending[2] = {false, false};  // ev_chain[e] marks the last chain that read eblocks[e]
+    bool side_pending = false;               // ev_done marks energy sums the system's stream has not joined
     DevBuf<double> out;  // [0] pe, [1] virial, [2] inside
     DevBuf<unsigned long long> inside_count;
     DevBuf<long long> fx_acc;  // fixed-point accumulators of the float kernels: pe, virial
@@ -638,7 +642,7 @@ md_status join_energy(md_forcefield* ff, md_system* s) {
 
 // The stream on which ff->out is final after the last force call: the second stream while its sums are pending
 cudaStream_t energy_stream(const md_forcefield* ff, const md_system* s) {
-    return ff->side_pending ? ff->side : s->stream;
+    return ff->side_pending ? ff->chain : s->stream;
 }
 
 // With fuse_drift (float modes on a tiled list, with the closing kick) the kernel also performs the next step's
@@ -661,24 +665,30 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
         const int b = ff->ew_next;
         if (want_energy && nb > 0) {
             if (!ff->side) {
-                MD_CUDA(cudaStreamCreateWithFlags(&ff->side, cudaStreamNonBlocking));
-                for (cudaEvent_t* e : {&ff->ev_force, &ff->ev_done, &ff->ev_read[0], &ff->ev_read[1]})
+                int least = 0, greatest = 0;
+                MD_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+                MD_CUDA(cudaStreamCreateWithPriority(&ff->side, cudaStreamNonBlocking, greatest));
+                MD_CUDA(cudaStreamCreateWithPriority(&ff->chain, cudaStreamNonBlocking, greatest));
+                for (cudaEvent_t* e : {&ff->ev_force, &ff->ev_done, &ff->ev_read[0], &ff->ev_read[1], &ff->ev_chain[0],
+                                       &ff->ev_chain[1]})
                     MD_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
             }
-            if (ff->pair_ew[b].count < static_cast<size_t>(pairs) || ff->eblocks.count < static_cast<size_t>(nb)) {
+            if (ff->pair_r2[b].count < static_cast<size_t>(pairs) || ff->eblocks[0].count < static_cast<size_t>(nb) ||
+                ff->eblocks[1].count < static_cast<size_t>(nb)) {
                 // a buffer is about to be replaced: no sums may read it; grow with headroom, since the pair count
                 // drifts up and down from one rebuild to the next
                 MD_CUDA(cudaStreamSynchronize(ff->side));
-                MD_CUDA(ff->pair_ew[b].reserve(static_cast<size_t>(pairs + pairs / 8)));
-                MD_CUDA(ff->eblocks.reserve(static_cast<size_t>(nb + nb / 8 + 1)));
+                MD_CUDA(cudaStreamSynchronize(ff->chain));
+                MD_CUDA(ff->pair_r2[b].reserve(static_cast<size_t>(pairs + pairs / 8)));
+                for (DevBuf<double2>& e : ff->eblocks) MD_CUDA(e.reserve(static_cast<size_t>(nb + nb / 8 + 1)));
             }
             if (ff->read_pending[b]) MD_CUDA(cudaStreamWaitEvent(s->stream, ff->ev_read[b], 0));
         }
         if (n > 0) {
             // variant 0: global gathers; 1: shared-memory tile; 2: global gathers a quad of entries at a time,
-            // branch-free (all bit-identical). With want_energy the kernel also stores every own pair's (E, W) in
+            // branch-free (all bit-identical). With want_energy the kernel also stores every own pair's r^2 in
             // pair order for the blocked sums below.
-            auto launch = [&](int variant, bool kick, double2* ew) -> md_status {
+            auto launch = [&](int variant, bool kick, double* ew) -> md_status {
                 if (variant == 1) {
                     const TileGeom& tg = nl->tiles_geom;
                     const size_t smem = sizeof(double4) * tg.max_staged;
@@ -703,23 +713,29 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
             MD_CUDA(cudaMemsetAsync(ff->inside_count.p, 0, sizeof(unsigned long long), s->stream));
             MD_TRY(profile_mark(s));
             MD_TRY(launch(nl->variant[MD_PREC_FP64], kick_dt > 0.0,
-                          want_energy && nb > 0 ? ff->pair_ew[b].p : nullptr));
+                          want_energy && nb > 0 ? ff->pair_r2[b].p : nullptr));
             MD_TRY(profile_mark(s));
         }
         if (want_energy) {
             if (nb > 0) {
-                // the ordered sums on the second stream, after this step's force kernel; the next step goes on
+                // the ordered sums on the side streams, after this step's force kernel; the next step goes on
+                const int eb = ff->eb_next;
                 MD_CUDA(cudaEventRecord(ff->ev_force, s->stream));
                 MD_CUDA(cudaStreamWaitEvent(ff->side, ff->ev_force, 0));
+                if (ff->chain_pending[eb]) MD_CUDA(cudaStreamWaitEvent(ff->side, ff->ev_chain[eb], 0));
                 k_pair_block_sums<<<blocks_for(nb, 32 * kPairSumWarps), 32 * kPairSumWarps, 0, ff->side>>>(
-                    ff->pair_ew[b].p, pairs, ff->eblocks.p, nb);
+                    ff->pair_r2[b].p, pairs, ff->lj, ff->eblocks[eb].p, nb);
                 MD_CHECK_LAUNCH();
                 MD_CUDA(cudaEventRecord(ff->ev_read[b], ff->side));
                 ff->read_pending[b] = true;
                 ff->ew_next = b ^ 1;
-                k_sum_blocks<<<1, 32, 0, ff->side>>>(ff->eblocks.p, nb, ff->out.p);
+                MD_CUDA(cudaStreamWaitEvent(ff->chain, ff->ev_read[b], 0));
+                k_sum_blocks<<<1, 32, 0, ff->chain>>>(ff->eblocks[eb].p, nb, ff->out.p);
                 MD_CHECK_LAUNCH();
-                MD_CUDA(cudaEventRecord(ff->ev_done, ff->side));
+                MD_CUDA(cudaEventRecord(ff->ev_chain[eb], ff->chain));
+                ff->chain_pending[eb] = true;
+                ff->eb_next = eb ^ 1;
+                MD_CUDA(cudaEventRecord(ff->ev_done, ff->chain));
                 ff->side_pending = true;
             } else {
                 MD_TRY(join_energy(ff, s));
@@ -1362,9 +1378,11 @@ md_status md_forcefield_destroy(md_forcefield* ff) {
     if (ff && ff->host_out) cudaFreeHost(ff->host_out);
     if (ff && ff->side) {
         cudaStreamSynchronize(ff->side);
-        for (cudaEvent_t e : {ff->ev_force, ff->ev_done, ff->ev_read[0], ff->ev_read[1]})
+        cudaStreamSynchronize(ff->chain);
+        for (cudaEvent_t e : {ff->ev_force, ff->ev_done, ff->ev_read[0], ff->ev_read[1], ff->ev_chain[0], ff->ev_chain[1]})
             if (e) cudaEventDestroy(e);
         cudaStreamDestroy(ff->side);
+        cudaStreamDestroy(ff->chain);
     }
     delete ff;
     return MD_OK;

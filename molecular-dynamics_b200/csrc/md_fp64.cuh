@@ -14,23 +14,23 @@ namespace md {
 // index. Pairs outside the cutoff contribute an exact zero in the reference and are skipped here. The
 // inside-cutoff count is the number of own pairs with r^2 < r_c^2 (a sum of whole numbers, exact).
 // With kick_vel set it also applies the closing half kick, v += (half_dt F) / m, with k_kick's sequence.
-// With pair_ew set, own pair s of particle i also stores (pairEnergy, pairVirial) at pair_ew[half_off[i] + s]:
-// E and (F/r) r^2 inside the cutoff, (0, 0) outside (src/Forcefield.cpp:288-296), for k_pair_block_sums.
-__device__ __forceinline__ void store_pair_ew(double2* pair_ew, long long k, bool in, double f, double e, double r2) {
-    pair_ew[k] = in ? make_double2(e, dmul(f, r2)) : make_double2(0.0, 0.0);
-}
+// With pair_r2 set, own pair s of particle i also stores its r^2 at pair_r2[half_off[i] + s], from which
+// k_pair_block_sums recomputes (pairEnergy, pairVirial) with the same pair_terms call: E and (F/r) r^2 inside the
+// cutoff, (0, 0) outside (src/Forcefield.cpp:288-296). One double per pair instead of the two terms halves the
+// records' traffic, and the recomputed terms are the same bits (the same operations on the same r^2).
+__device__ __forceinline__ void store_pair_r2(double* pair_r2, long long k, double r2) { pair_r2[k] = r2; }
 
 __global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ lj, const uint32_t* __restrict__ rows,
                              int cap, const int2* __restrict__ counts, double* __restrict__ force,
                              unsigned long long* __restrict__ inside, double* __restrict__ kick_vel,
                              const double* __restrict__ mass, double half_dt, const long long* __restrict__ half_off,
-                             double2* __restrict__ pair_ew) {
+                             double* __restrict__ pair_r2) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long ins = 0;
     if (i < n) {
         const double4 pi = pos[i];
         const int2 c = counts[i];
-        const long long pb = pair_ew ? half_off[i] : 0;
+        const long long pb = pair_r2 ? half_off[i] : 0;
         double fx = 0.0, fy = 0.0, fz = 0.0;
         for (int s = 0; s < c.x; ++s) {
             const double4 pj = pos[rows[row_index(i, s, cap)] & kIndexMask];
@@ -39,12 +39,12 @@ __global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ
             const double dz = min_image(dsub(pi.z, pj.z), box);
             const double r2 = norm2(dx, dy, dz);
             if (!(r2 < lj.rc2)) {
-                if (pair_ew) store_pair_ew(pair_ew, pb + s, false, 0.0, 0.0, r2);
+                if (pair_r2) store_pair_r2(pair_r2, pb + s, r2);
                 continue;
             }
             double f, e;
             pair_terms(r2, lj, f, e);
-            if (pair_ew) store_pair_ew(pair_ew, pb + s, true, f, e, r2);
+            if (pair_r2) store_pair_r2(pair_r2, pb + s, r2);
             fx = dadd(fx, dmul(f, dx));
             fy = dadd(fy, dmul(f, dy));
             fz = dadd(fz, dmul(f, dz));
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(128) k_force_fp64_quads(const double4* __restr
                                                           unsigned long long* __restrict__ inside,
                                                           double* __restrict__ kick_vel, const double* __restrict__ mass,
                                                           double half_dt, const long long* __restrict__ half_off,
-                                                          double2* __restrict__ pair_ew) {
+                                                          double* __restrict__ pair_r2) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long ins = 0;
     if (i < n) {
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(128) k_force_fp64_quads(const double4* __restr
         const int2 c = counts[i];
         const int m = c.x + c.y;
         const int quads = (m + 3) >> 2;
-        const long long pb = pair_ew ? half_off[i] : 0;
+        const long long pb = pair_r2 ? half_off[i] : 0;
         double fx = 0.0, fy = 0.0, fz = 0.0;
         const uint4* rq = reinterpret_cast<const uint4*>(rows) + static_cast<size_t>(i >> 5) * (cap >> 2) * 32 + (i & 31);
         uint4 nq = make_uint4(0, 0, 0, 0);
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(128) k_force_fp64_quads(const double4* __restr
                 fz = dadd(fz, in ? dmul(f, dz) : 0.0);
                 if (sl < c.x) {
                     ins += in ? 1u : 0u;
-                    if (pair_ew) store_pair_ew(pair_ew, pb + sl, in, f, e, r2);
+                    if (pair_r2) store_pair_r2(pair_r2, pb + sl, r2);
                 }
             }
         }
@@ -141,19 +141,21 @@ __global__ void __launch_bounds__(128) k_force_fp64_quads(const double4* __restr
 
 constexpr int kEnergyWarps = 4;  // warps per block of the blocked kinetic-energy sums
 
-// The inner loop of deterministicSum (include/Parallel.hpp:43-46) over the (pairEnergy, pairVirial) array the
-// force kernel stored: block b sums pairs [1024 b, 1024 b + 1024) from 0.0 one after another. One lane per
-// block, so a warp advances 32 blocks' ordered sums together; the warp stages 32 consecutive records of each of
-// its blocks in shared memory at a time (coalesced 512-byte loads), and each lane then adds its block's 32.
-constexpr int kPairSumWarps = 2;
-__global__ void __launch_bounds__(32 * kPairSumWarps) k_pair_block_sums(const double2* __restrict__ pair_ew,
-                                                                        long long pairs,
+// The inner loop of deterministicSum (include/Parallel.hpp:43-46) over the (pairEnergy, pairVirial) array, whose
+// terms are recomputed here from the r^2 records the force kernel stored: block b sums pairs
+// [1024 b, 1024 b + 1024) from 0.0 one after another, a pair outside the cutoff adding 0.0 as the reference's
+// zero entries do. One lane per block, so a warp advances 32 blocks' ordered sums together; the warp stages 32
+// consecutive records of each of its blocks in shared memory at a time (coalesced 256-byte loads), and each lane
+// then evaluates and adds its block's 32 (the evaluations are independent of the sums, so they overlap).
+constexpr int kPairSumWarps = 4;
+__global__ void __launch_bounds__(32 * kPairSumWarps) k_pair_block_sums(const double* __restrict__ pair_r2,
+                                                                        long long pairs, LJ lj,
                                                                         double2* __restrict__ block_sums, int nblocks) {
-    __shared__ double2 tile[kPairSumWarps][32][33];
+    __shared__ double tile[kPairSumWarps][32][33];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b0 = (blockIdx.x * kPairSumWarps + warp) * 32;  // this warp's first block
     if (b0 >= nblocks) return;
-    double2(*t)[33] = tile[warp];
+    double(*t)[33] = tile[warp];
     const int b = b0 + lane;
     const long long k0 = static_cast<long long>(b) * kChunk;
     const int m = b < nblocks ? static_cast<int>(pairs - k0 < kChunk ? pairs - k0 : kChunk) : 0;
@@ -162,14 +164,18 @@ __global__ void __launch_bounds__(32 * kPairSumWarps) k_pair_block_sums(const do
         __syncwarp();
         for (int r = 0; r < 32; ++r) {  // row r: records [c, c + 32) of block b0 + r, lane = record
             const long long k = static_cast<long long>(b0 + r) * kChunk + c + lane;
-            t[r][lane] = b0 + r < nblocks && k < pairs ? pair_ew[k] : make_double2(0.0, 0.0);
+            t[r][lane] = b0 + r < nblocks && k < pairs ? __ldcs(pair_r2 + k) : lj.rc2;
         }
         __syncwarp();
         const int e = m - c < 32 ? m - c : 32;
+#pragma unroll 4
         for (int u = 0; u < e; ++u) {
-            const double2 x = t[lane][u];
-            se = dadd(se, x.x);
-            sw = dadd(sw, x.y);
+            const double r2 = t[lane][u];
+            const bool in = r2 < lj.rc2;
+            double f, en;
+            pair_terms(in ? r2 : 1.0, lj, f, en);
+            se = dadd(se, in ? en : 0.0);
+            sw = dadd(sw, in ? dmul(f, r2) : 0.0);
         }
     }
     if (b < nblocks) block_sums[b] = make_double2(se, sw);

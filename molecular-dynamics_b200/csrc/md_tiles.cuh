@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(kTileThreads) k_force_fp64_tile(
     const double4* __restrict__ pos, int n_atoms, const int* __restrict__ cell_start,
     const int* __restrict__ cell_sorted, TileGeom g, LJ lj, const uint32_t* __restrict__ rows, int cap,
     const int2* __restrict__ counts, double* __restrict__ force, unsigned long long* __restrict__ inside,
-    KickArgs kick, const long long* __restrict__ half_off, double2* __restrict__ pair_ew) {
+    KickArgs kick, const long long* __restrict__ half_off, double* __restrict__ pair_r2) {
     extern __shared__ double4 s_p[];
     __shared__ TileTables t;
     __shared__ int s_delta[kMaxSegment][32];
@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(kTileThreads) k_force_fp64_tile(
         const int* delta = s_delta[h];
         const double4 pi = s_p[i + delta[13]];  // code 13 = (0, 0, 0): the home cell
         const int2 c = counts[i];
-        const long long pb = pair_ew ? half_off[i] : 0;
+        const long long pb = pair_r2 ? half_off[i] : 0;
         double fx = 0.0, fy = 0.0, fz = 0.0;
         for (int s = 0; s < c.x + c.y; ++s) {
             const uint32_t e = rows[row_index(i, s, cap)];
@@ -452,13 +452,13 @@ __global__ void __launch_bounds__(kTileThreads) k_force_fp64_tile(
             const double dz = min_image(dsub(a.z, b.z), g.box);
             const double r2 = norm2(dx, dy, dz);
             if (!(r2 < lj.rc2)) {
-                if (own && pair_ew) store_pair_ew(pair_ew, pb + s, false, 0.0, 0.0, r2);
+                if (own && pair_r2) store_pair_r2(pair_r2, pb + s, r2);
                 continue;
             }
             double f, en;
             pair_terms(r2, lj, f, en);
             if (own) {
-                if (pair_ew) store_pair_ew(pair_ew, pb + s, true, f, en, r2);
+                if (pair_r2) store_pair_r2(pair_r2, pb + s, r2);
                 fx = dadd(fx, dmul(f, dx));
                 fy = dadd(fy, dmul(f, dy));
                 fz = dadd(fz, dmul(f, dz));
