@@ -578,14 +578,14 @@ def run_gpu_arm(a):
     # DRAM bytes per atom of one force launch: the particle's own coordinates, its force, the full-list int32
     # indices (neighbour coordinates are gathered through L1/L2 and counted once, in the own term), the fused
     # closing kick (velocity read and write, mass) and, in the float modes, the fused next kick and drift
-    # (position in and out, reference position, build cell, new float frame); FP64 adds its own-pair (E, W)
+    # (position in and out, reference position, build cell, new float frame); FP64 adds its own-pair r^2
     # records for the ordered energy sums.
     own = 32 if a.precision == "fp64" else 16
     bytes_per_atom = own + 24 + 4 * 2 * pairs / n + 56
     if a.precision in ("fp32fx", "fp32", "fx32", "fx64"):
         bytes_per_atom += 32 + 32 + 4 + 32 + 16
     if a.precision == "fp64":
-        bytes_per_atom += 16 * pairs / n
+        bytes_per_atom += 8 * pairs / n
     achieved = bytes_per_atom * n / kernel_s / 1e9
     if a.precision == "fx32":
         bytes_per_atom += 32  # the own fixed-point frame read and the next one written, beside the float frames

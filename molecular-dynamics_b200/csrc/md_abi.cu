@@ -630,7 +630,7 @@ md_status choose_variant(md_system* s, md_nlist* nl, int prec, Launch&& launch) 
 // them). Returns through *fused_ke whether the fused kick also left the step's kinetic energy in
 // s->scal[kScalKE] (float tile kernels only; fixed-point, not the reference's summation order).
 md_status kick_async(md_system* s, double dt);
-// The system's stream waits for the FP64 energy sums queued on the force field's second stream (every reader or
+// The system's stream waits for the FP64 energy sums queued on the force field's side streams (every reader or
 // writer of ff->out on the system's stream calls this first)
 md_status join_energy(md_forcefield* ff, md_system* s) {
     if (ff->side_pending) {
@@ -640,7 +640,7 @@ md_status join_energy(md_forcefield* ff, md_system* s) {
     return MD_OK;
 }
 
-// The stream on which ff->out is final after the last force call: the second stream while its sums are pending
+// The stream on which ff->out is final after the last force call: the chain stream while its sums are pending
 cudaStream_t energy_stream(const md_forcefield* ff, const md_system* s) {
     return ff->side_pending ? ff->chain : s->stream;
 }
@@ -661,7 +661,7 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
         if (n > 0) MD_TRY(ensure_pairs(nl));
         const long long pairs = n > 0 ? static_cast<long long>(nl->pairs) : 0;
         const int nb = static_cast<int>((pairs + kChunk - 1) / kChunk);
-        // the (E, W) buffer this step fills: free once the sums that last read it are done
+        // the r^2 record buffer this step fills: free once the block sums that last read it are done
         const int b = ff->ew_next;
         if (want_energy && nb > 0) {
             if (!ff->side) {

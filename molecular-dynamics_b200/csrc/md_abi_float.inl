@@ -512,7 +512,7 @@ md_status run_steps(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, in
         const bool fixed_fresh = drifted && !rebuilt;
         MD_TRY(forces_list_async(ff, s, nl, want_energy, dt, true, &fused_ke, fuse, fixed_fresh));
         drifted = fuse;
-        if (want_energy) {  // on the stream where this step's sums end (FP64: the force field's second stream)
+        if (want_energy) {  // on the stream where this step's sums end (FP64: the force field's chain stream)
             const cudaStream_t es = energy_stream(ff, s);
             MD_CUDA(cudaMemcpyAsync(rec.p + 3 * k, ff->out.p, 2 * sizeof(double), cudaMemcpyDeviceToDevice, es));
             if (es != s->stream) MD_CUDA(cudaEventRecord(ff->ev_done, es));  // the join covers the copy too
