@@ -537,6 +537,12 @@ def run_gpu_arm(a):
         ff2 = md.LennardJonesForceField(1.0, 1.0, 2.5, precision=prec)
         st2 = torch.cuda.ExternalStream(s2.stream)
         x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        # one untimed pass, as a caller's first call: it allocates the system's, list's and force field's device
+        # buffers and captures the run's graphs, which later calls reuse
+        s2.upload(pos=h_pos.numpy(), vel=h_vel.numpy(), mass=h_mass.numpy())
+        nl2.build(s2)
+        ff2.compute_forces(s2, nl2)
+        integ.prepare(s2, ff2, nl2, a.steps)
         if dist:
             dist.barrier()
         s2.synchronize()
@@ -558,7 +564,8 @@ def run_gpu_arm(a):
         e2e = {"value": replica_throughput(world, n, a.steps, ems), "unit": "atom-steps/s",
                "h2d_bytes_per_step": h2d / a.steps, "d2h_bytes_per_step": d2h / a.steps,
                "includes": "pinned H2D of positions/velocities/masses, list build, initial forces, all steps with "
-                           "per-step PE/KE/virial read back, D2H of final positions/velocities"}
+                           "per-step PE/KE/virial read back, D2H of final positions/velocities (after one untimed "
+                           "pass that allocated the device buffers and captured the run's graphs)"}
         del s2, nl2, ff2
 
     replicas = replica_workload(md, a, local) if rank == 0 and a.replica_steps > 0 else None

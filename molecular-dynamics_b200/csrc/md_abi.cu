@@ -673,13 +673,16 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
                                        &ff->ev_chain[1]})
                     MD_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
             }
-            if (ff->pair_r2[b].count < static_cast<size_t>(pairs) || ff->eblocks[0].count < static_cast<size_t>(nb) ||
-                ff->eblocks[1].count < static_cast<size_t>(nb)) {
-                // a buffer is about to be replaced: no sums may read it; grow with headroom, since the pair count
+            const auto small = [&](size_t r2, size_t blocks) {
+                return r2 < static_cast<size_t>(pairs) || blocks < static_cast<size_t>(nb);
+            };
+            if (small(ff->pair_r2[0].count, ff->eblocks[0].count) || small(ff->pair_r2[1].count, ff->eblocks[1].count)) {
+                // buffers are about to be replaced: no sums may read them; both pairs grow together (so that the
+                // second buffer is not allocated in the middle of a run), with headroom, since the pair count
                 // drifts up and down from one rebuild to the next
                 MD_CUDA(cudaStreamSynchronize(ff->side));
                 MD_CUDA(cudaStreamSynchronize(ff->chain));
-                MD_CUDA(ff->pair_r2[b].reserve(static_cast<size_t>(pairs + pairs / 8)));
+                for (DevBuf<double>& r : ff->pair_r2) MD_CUDA(r.reserve(static_cast<size_t>(pairs + pairs / 8)));
                 for (DevBuf<double2>& e : ff->eblocks) MD_CUDA(e.reserve(static_cast<size_t>(nb + nb / 8 + 1)));
             }
             if (ff->read_pending[b]) MD_CUDA(cudaStreamWaitEvent(s->stream, ff->ev_read[b], 0));
