@@ -210,15 +210,16 @@ md_status md_step_all_pairs(md_system* s, md_forcefield* ff, double dt, double* 
 /* n_steps list steps (md_sim's loops, src/main.cpp:219-304). Per step, in order: step_list; then the optional
  * thermostat; then the optional g(r) sample. Outputs (each NULL or n_steps long, host memory): pe[k] the step's
  * PE, ke[k] the kinetic energy after the thermostat, virial[k].
- * The float precisions on a list with shared-memory tiles run as CUDA graphs of up to md_system_set_graph's
- * chunk length (64 steps by default) when the run is at least two chunks long or md_run_prepare captured the
- * graphs for its length: every step, the thermostat and the g(r) sample included, is in the graph,
+ * On a list with shared-memory tiles a run executes as CUDA graphs of up to md_system_set_graph's chunk length
+ * (64 steps by default) when it is at least two chunks long or md_run_prepare captured the graphs for its length:
+ * every step, the thermostat, the g(r) sample and MD_PREC_FP64's ordered energy sums included, is in the graph,
  * and a list rebuild is decided on the device (a conditional node runs the rebuild when the half-skin test of the
- * step's drift flagged a particle), so the host waits once per chunk. A rebuild that outgrows the row capacity or
- * the recorded shared-memory tile makes the library run that chunk again on the host path from the chunk's
- * starting state, growing what it must; results are the same bits either way. MD_PREC_FP64 (whose ordered
- * energy sums need the pair count after each rebuild on the host), small boxes and lists pinned to the global
- * build take the host-driven loop, which reads the half-skin flag after each drift. */
+ * step's drift flagged a particle), so the host waits once per chunk. A rebuild that outgrows the row capacity,
+ * the recorded shared-memory tile or (MD_PREC_FP64) the energy records' buffers makes the library run that chunk
+ * again on the host path from the chunk's starting state, growing what it must; results are the same bits either
+ * way. MD_PREC_FP64 systems of more than 10^6 particles (whose ordered energy sums overlap the next steps better
+ * on their own streams), small boxes and lists pinned to the global build take the host-driven loop, which reads
+ * the half-skin flag after each drift. */
 typedef struct md_run_options {
     int thermostat;             /* 0 none (NVE), 1 rescale, 2 Bussi */
     int rescale_every;          /* rescale when (first_step + k) % rescale_every == 0 */

@@ -260,6 +260,9 @@ struct md_forcefield {
     // priority, so that their blocks are not queued behind the next step's force kernel.
     DevBuf<double> pair_r2[2];
     DevBuf<double2> eblocks[2];
+    DevBuf<long long> epairs;   // [b]: the pair count of the records in pair_r2[b], copied when the step fills them
+    DevBuf<int> enblocks;       // [e]: the block count of eblocks[e]
+    int side_priority = 0;      // of the two streams (the device's highest), also given to their kernels in graphs
     int ew_next = 0, eb_next = 0;
     cudaStream_t side = nullptr, chain = nullptr;
     cudaEvent_t ev_force = nullptr, ev_done = nullptr, ev_read[2] = {nullptr, nullptr}, ev_chain[2] = {nullptr, nullptr};
@@ -630,6 +633,67 @@ md_status choose_variant(md_system* s, md_nlist* nl, int prec, Launch&& launch) 
 // them). Returns through *fused_ke whether the fused kick also left the step's kinetic energy in
 // s->scal[kScalKE] (float tile kernels only; fixed-point, not the reference's summation order).
 md_status kick_async(md_system* s, double dt);
+// Lists with fewer pairs than this keep each pair's (E, W) for the FP64 energy sums, larger ones its r^2
+// (store_pair_rec)
+constexpr long long kTermsMaxPairs = 4'000'000;
+
+// A kernel launch carrying a scheduling priority: the launch keeps it when a CUDA graph records it (a graph's
+// nodes do not take the priority of the stream they were captured from)
+template <typename... P, typename... A>
+md_status launch_priority(void (*kernel)(P...), unsigned grid, unsigned block, cudaStream_t st, int priority,
+                          A&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = priority;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    MD_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
+    MD_CHECK_LAUNCH();
+    return MD_OK;
+}
+
+// The FP64 energy sums' two streams and their events, created on the first force call that records energies
+md_status energy_streams(md_forcefield* ff) {
+    int least = 0, greatest = 0;
+    MD_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    MD_CUDA(cudaStreamCreateWithPriority(&ff->side, cudaStreamNonBlocking, greatest));
+    MD_CUDA(cudaStreamCreateWithPriority(&ff->chain, cudaStreamNonBlocking, greatest));
+    ff->side_priority = greatest;
+    for (cudaEvent_t* e : {&ff->ev_force, &ff->ev_done, &ff->ev_read[0], &ff->ev_read[1], &ff->ev_chain[0],
+                           &ff->ev_chain[1]})
+        MD_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    MD_CUDA(ff->epairs.reserve(2));
+    MD_CUDA(ff->enblocks.reserve(2));
+    return MD_OK;
+}
+
+// Waits for every energy sum queued on the two streams; afterwards no buffer is being read and the buffers are used
+// from the first pair again (what a CUDA graph's capture starts from and what its run leaves behind)
+md_status energy_quiesce(md_forcefield* ff) {
+    if (ff->side) {
+        MD_CUDA(cudaStreamSynchronize(ff->side));
+        MD_CUDA(cudaStreamSynchronize(ff->chain));
+    }
+    ff->read_pending[0] = ff->read_pending[1] = false;
+    ff->chain_pending[0] = ff->chain_pending[1] = false;
+    ff->side_pending = false;
+    ff->ew_next = ff->eb_next = 0;
+    return MD_OK;
+}
+
+// Both pairs of energy buffers for at least `pairs` pair records of either form (two doubles each; call with
+// nothing queued on the streams)
+md_status reserve_energy_records(md_forcefield* ff, long long pairs) {
+    const size_t blocks = static_cast<size_t>((pairs + kChunk - 1) / kChunk) + 1;
+    for (DevBuf<double>& r : ff->pair_r2) MD_CUDA(r.reserve(2 * static_cast<size_t>(pairs)));
+    for (DevBuf<double2>& e : ff->eblocks) MD_CUDA(e.reserve(blocks));
+    return MD_OK;
+}
+
 // The system's stream waits for the FP64 energy sums queued on the force field's side streams (every reader or
 // writer of ff->out on the system's stream calls this first)
 md_status join_energy(md_forcefield* ff, md_system* s) {
@@ -658,83 +722,98 @@ md_status forces_list_async(md_forcefield* ff, md_system* s, md_nlist* nl, bool 
     MD_CUDA(ff->inside_count.reserve(1));
     MD_CUDA(cudaMemsetAsync(ff->inside_count.p, 0, sizeof(unsigned long long), s->stream));
     if (ff->precision == MD_PREC_FP64) {
-        if (n > 0) MD_TRY(ensure_pairs(nl));
-        const long long pairs = n > 0 ? static_cast<long long>(nl->pairs) : 0;
+        // Inside a CUDA graph's capture (g_capturing) the pair count of a list the graph rebuilt is known only on
+        // the device (half_off[n]): the buffers were sized before the capture (graph_prepare_buffers), the record
+        // stores stop at their size, and the sums read the count from the device.
+        const bool capturing = g_capturing;
+        if (n > 0 && !capturing) MD_TRY(ensure_pairs(nl));
+        const long long pairs = n > 0 && !capturing ? static_cast<long long>(nl->pairs) : 0;
         const int nb = static_cast<int>((pairs + kChunk - 1) / kChunk);
         // the r^2 record buffer this step fills: free once the block sums that last read it are done
         const int b = ff->ew_next;
-        if (want_energy && nb > 0) {
-            if (!ff->side) {
-                int least = 0, greatest = 0;
-                MD_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-                MD_CUDA(cudaStreamCreateWithPriority(&ff->side, cudaStreamNonBlocking, greatest));
-                MD_CUDA(cudaStreamCreateWithPriority(&ff->chain, cudaStreamNonBlocking, greatest));
-                for (cudaEvent_t* e : {&ff->ev_force, &ff->ev_done, &ff->ev_read[0], &ff->ev_read[1], &ff->ev_chain[0],
-                                       &ff->ev_chain[1]})
-                    MD_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-            }
-            const auto small = [&](size_t r2, size_t blocks) {
-                return r2 < static_cast<size_t>(pairs) || blocks < static_cast<size_t>(nb);
-            };
-            if (small(ff->pair_r2[0].count, ff->eblocks[0].count) || small(ff->pair_r2[1].count, ff->eblocks[1].count)) {
-                // buffers are about to be replaced: no sums may read them; both pairs grow together (so that the
-                // second buffer is not allocated in the middle of a run), with headroom, since the pair count
-                // drifts up and down from one rebuild to the next
-                MD_CUDA(cudaStreamSynchronize(ff->side));
-                MD_CUDA(cudaStreamSynchronize(ff->chain));
-                for (DevBuf<double>& r : ff->pair_r2) MD_CUDA(r.reserve(static_cast<size_t>(pairs + pairs / 8)));
-                for (DevBuf<double2>& e : ff->eblocks) MD_CUDA(e.reserve(static_cast<size_t>(nb + nb / 8 + 1)));
+        const bool sums = want_energy && (capturing ? n > 0 : nb > 0);
+        if (sums) {
+            if (!capturing) {
+                if (!ff->side) MD_TRY(energy_streams(ff));
+                const auto small = [&](size_t r2, size_t blocks) {
+                    return r2 < 2 * static_cast<size_t>(pairs) || blocks < static_cast<size_t>(nb);
+                };
+                if (small(ff->pair_r2[0].count, ff->eblocks[0].count) ||
+                    small(ff->pair_r2[1].count, ff->eblocks[1].count)) {
+                    // buffers are about to be replaced: no sums may read them; both pairs grow together (so that
+                    // the second buffer is not allocated in the middle of a run), with headroom, since the pair
+                    // count drifts up and down from one rebuild to the next
+                    MD_TRY(energy_quiesce(ff));
+                    MD_TRY(reserve_energy_records(ff, pairs + pairs / 8));
+                }
             }
             if (ff->read_pending[b]) MD_CUDA(cudaStreamWaitEvent(s->stream, ff->ev_read[b], 0));
         }
+        const long long rec_cap = sums ? static_cast<long long>(ff->pair_r2[b].count / 2) : 0;
+        const bool terms = (capturing ? rec_cap : pairs) < kTermsMaxPairs;  // the records' form
         if (n > 0) {
             // variant 0: global gathers; 1: shared-memory tile; 2: global gathers a quad of entries at a time,
             // branch-free (all bit-identical). With want_energy the kernel also stores every own pair's r^2 in
             // pair order for the blocked sums below.
-            auto launch = [&](int variant, bool kick, double* ew) -> md_status {
+            auto launch_form = [&](int variant, bool kick, double* ew, auto form) -> md_status {
+                constexpr bool kTerms = decltype(form)::value;
                 if (variant == 1) {
                     const TileGeom& tg = nl->tiles_geom;
                     const size_t smem = sizeof(double4) * tg.max_staged;
-                    MD_CUDA(allow_smem(k_force_fp64_tile, smem));
+                    MD_CUDA(allow_smem(k_force_fp64_tile<kTerms>, smem));
                     const KickArgs ka{kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt};
-                    k_force_fp64_tile<<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
+                    k_force_fp64_tile<kTerms><<<tile_blocks(tg), kTileThreads, smem, s->stream>>>(
                         s->pos.p, n, nl->grid.start.p, nl->cell_sorted.p, tg, ff->lj, nl->rows.p, nl->cap,
-                        nl->counts.p, s->force.p, ff->inside_count.p, ka, nl->half_off.p, ew);
+                        nl->counts.p, s->force.p, ff->inside_count.p, ka, nl->half_off.p, ew, rec_cap);
                 } else if (variant == 2) {
-                    k_force_fp64_quads<<<blocks_for(n, 128), 128, 0, s->stream>>>(
+                    k_force_fp64_quads<kTerms><<<blocks_for(n, 128), 128, 0, s->stream>>>(
                         s->pos.p, n, s->box, ff->lj, nl->rows.p, nl->cap, nl->counts.p, s->force.p, ff->inside_count.p,
-                        kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt, nl->half_off.p, ew);
+                        kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt, nl->half_off.p, ew, rec_cap);
                 } else {
-                    k_force_fp64<<<blocks_for(n, 128), 128, 0, s->stream>>>(
+                    k_force_fp64<kTerms><<<blocks_for(n, 128), 128, 0, s->stream>>>(
                         s->pos.p, n, s->box, ff->lj, nl->rows.p, nl->cap, nl->counts.p, s->force.p, ff->inside_count.p,
-                        kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt, nl->half_off.p, ew);
+                        kick ? s->vel.p : nullptr, s->mass.p, 0.5 * kick_dt, nl->half_off.p, ew, rec_cap);
                 }
                 MD_CHECK_LAUNCH();
                 return MD_OK;
             };
+            auto launch = [&](int variant, bool kick, double* ew) -> md_status {
+                return terms ? launch_form(variant, kick, ew, std::true_type{})
+                             : launch_form(variant, kick, ew, std::false_type{});
+            };
             MD_TRY(choose_variant(s, nl, MD_PREC_FP64, [&](int v) { return launch(v, false, nullptr); }));
             MD_CUDA(cudaMemsetAsync(ff->inside_count.p, 0, sizeof(unsigned long long), s->stream));
             MD_TRY(profile_mark(s));
-            MD_TRY(launch(nl->variant[MD_PREC_FP64], kick_dt > 0.0,
-                          want_energy && nb > 0 ? ff->pair_r2[b].p : nullptr));
+            MD_TRY(launch(nl->variant[MD_PREC_FP64], kick_dt > 0.0, sums ? ff->pair_r2[b].p : nullptr));
             MD_TRY(profile_mark(s));
         }
         if (want_energy) {
-            if (nb > 0) {
+            if (sums) {
                 // the ordered sums on the side streams, after this step's force kernel; the next step goes on
                 const int eb = ff->eb_next;
+                const int grid_blocks = capturing ? static_cast<int>((rec_cap + kChunk - 1) / kChunk) : nb;
+                // this step's pair count, kept with its records (a rebuild for the next step rewrites half_off)
+                MD_CUDA(cudaMemcpyAsync(ff->epairs.p + b, nl->half_off.p + n, sizeof(long long),
+                                        cudaMemcpyDeviceToDevice, s->stream));
                 MD_CUDA(cudaEventRecord(ff->ev_force, s->stream));
                 MD_CUDA(cudaStreamWaitEvent(ff->side, ff->ev_force, 0));
                 if (ff->chain_pending[eb]) MD_CUDA(cudaStreamWaitEvent(ff->side, ff->ev_chain[eb], 0));
-                k_pair_block_sums<<<blocks_for(nb, 32 * kPairSumWarps), 32 * kPairSumWarps, 0, ff->side>>>(
-                    ff->pair_r2[b].p, pairs, ff->lj, ff->eblocks[eb].p, nb);
-                MD_CHECK_LAUNCH();
+                if (terms)
+                    MD_TRY(launch_priority(k_pair_block_sums_terms, blocks_for(grid_blocks, 32 * kPairSumWarpsTerms),
+                                           32 * kPairSumWarpsTerms, ff->side, ff->side_priority,
+                                           reinterpret_cast<const double2*>(ff->pair_r2[b].p), ff->epairs.p + b,
+                                           rec_cap, ff->eblocks[eb].p, ff->enblocks.p + eb));
+                else
+                    MD_TRY(launch_priority(k_pair_block_sums, blocks_for(grid_blocks, 32 * kPairSumWarps),
+                                           32 * kPairSumWarps, ff->side, ff->side_priority, ff->pair_r2[b].p,
+                                           ff->epairs.p + b, rec_cap, ff->lj, ff->eblocks[eb].p,
+                                           ff->enblocks.p + eb));
                 MD_CUDA(cudaEventRecord(ff->ev_read[b], ff->side));
                 ff->read_pending[b] = true;
                 ff->ew_next = b ^ 1;
                 MD_CUDA(cudaStreamWaitEvent(ff->chain, ff->ev_read[b], 0));
-                k_sum_blocks<<<1, 32, 0, ff->chain>>>(ff->eblocks[eb].p, nb, ff->out.p);
-                MD_CHECK_LAUNCH();
+                MD_TRY(launch_priority(k_sum_pair_blocks, 1, 32, ff->chain, ff->side_priority, ff->eblocks[eb].p,
+                                       ff->enblocks.p + eb, ff->out.p));
                 MD_CUDA(cudaEventRecord(ff->ev_chain[eb], ff->chain));
                 ff->chain_pending[eb] = true;
                 ff->eb_next = eb ^ 1;

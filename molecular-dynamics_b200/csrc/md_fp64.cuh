@@ -14,17 +14,30 @@ namespace md {
 // index. Pairs outside the cutoff contribute an exact zero in the reference and are skipped here. The
 // inside-cutoff count is the number of own pairs with r^2 < r_c^2 (a sum of whole numbers, exact).
 // With kick_vel set it also applies the closing half kick, v += (half_dt F) / m, with k_kick's sequence.
-// With pair_r2 set, own pair s of particle i also stores its r^2 at pair_r2[half_off[i] + s], from which
-// k_pair_block_sums recomputes (pairEnergy, pairVirial) with the same pair_terms call: E and (F/r) r^2 inside the
-// cutoff, (0, 0) outside (src/Forcefield.cpp:288-296). One double per pair instead of the two terms halves the
-// records' traffic, and the recomputed terms are the same bits (the same operations on the same r^2).
-__device__ __forceinline__ void store_pair_r2(double* pair_r2, long long k, double r2) { pair_r2[k] = r2; }
+// With pair_r2 set, own pair s of particle i also stores its record for the ordered energy sums at index
+// half_off[i] + s: with `terms`, its (pairEnergy, pairVirial) as a double2, E and (F/r) r^2 inside the cutoff,
+// (0, 0) outside (src/Forcefield.cpp:288-296), which k_pair_block_sums_terms adds; without, its r^2, from which
+// k_pair_block_sums recomputes the two terms with the same pair_terms call (the same operations on the same r^2,
+// so the same bits). The r^2 record halves the traffic, which pays for large lists; for small ones the recomputation
+// lengthens the sums (each lane evaluates its block's 1024 pairs in turn), so they keep the terms. Records past
+// rec_cap, the buffer's size in records, are dropped: only a list rebuilt inside a CUDA graph can outgrow the
+// buffer, and the graph's run then reports the overflow and repeats its steps on the host path.
+template <bool kTerms>
+__device__ __forceinline__ void store_pair_rec(double* rec, long long k, double r2, double f, double e, bool in,
+                                               long long rec_cap) {
+    if (k >= rec_cap) return;
+    if (kTerms)
+        reinterpret_cast<double2*>(rec)[k] = in ? make_double2(e, dmul(f, r2)) : make_double2(0.0, 0.0);
+    else
+        rec[k] = r2;  // the energy term is then never used, and the compiler leaves it out
+}
 
+template <bool kTerms>
 __global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ lj, const uint32_t* __restrict__ rows,
                              int cap, const int2* __restrict__ counts, double* __restrict__ force,
                              unsigned long long* __restrict__ inside, double* __restrict__ kick_vel,
                              const double* __restrict__ mass, double half_dt, const long long* __restrict__ half_off,
-                             double* __restrict__ pair_r2) {
+                             double* __restrict__ pair_r2, long long rec_cap) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long ins = 0;
     if (i < n) {
@@ -39,12 +52,12 @@ __global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ
             const double dz = min_image(dsub(pi.z, pj.z), box);
             const double r2 = norm2(dx, dy, dz);
             if (!(r2 < lj.rc2)) {
-                if (pair_r2) store_pair_r2(pair_r2, pb + s, r2);
+                if (pair_r2) store_pair_rec<kTerms>(pair_r2, pb + s, r2, 0.0, 0.0, false, rec_cap);
                 continue;
             }
             double f, e;
             pair_terms(r2, lj, f, e);
-            if (pair_r2) store_pair_r2(pair_r2, pb + s, r2);
+            if (pair_r2) store_pair_rec<kTerms>(pair_r2, pb + s, r2, f, e, true, rec_cap);
             fx = dadd(fx, dmul(f, dx));
             fy = dadd(fy, dmul(f, dy));
             fz = dadd(fz, dmul(f, dz));
@@ -82,13 +95,14 @@ __global__ void k_force_fp64(const double4* __restrict__ pos, int n, Box box, LJ
 // odd (round() and the |d| <= L/4 shortcut are symmetric) and IEEE subtraction antisymmetric, so each sum sees
 // the reference's nonzero terms in the reference's order; a masked 0.0 leaves a sum unchanged because a sum
 // that starts at +0.0 never becomes -0.0.
+template <bool kTerms>
 __global__ void __launch_bounds__(128) k_force_fp64_quads(const double4* __restrict__ pos, int n, Box box, LJ lj,
                                                           const uint32_t* __restrict__ rows, int cap,
                                                           const int2* __restrict__ counts, double* __restrict__ force,
                                                           unsigned long long* __restrict__ inside,
                                                           double* __restrict__ kick_vel, const double* __restrict__ mass,
                                                           double half_dt, const long long* __restrict__ half_off,
-                                                          double* __restrict__ pair_r2) {
+                                                          double* __restrict__ pair_r2, long long rec_cap) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long ins = 0;
     if (i < n) {
@@ -123,7 +137,7 @@ __global__ void __launch_bounds__(128) k_force_fp64_quads(const double4* __restr
                 fz = dadd(fz, in ? dmul(f, dz) : 0.0);
                 if (sl < c.x) {
                     ins += in ? 1u : 0u;
-                    if (pair_r2) store_pair_r2(pair_r2, pb + sl, r2);
+                    if (pair_r2) store_pair_rec<kTerms>(pair_r2, pb + sl, r2, f, e, in, rec_cap);
                 }
             }
         }
@@ -148,10 +162,18 @@ constexpr int kEnergyWarps = 4;  // warps per block of the blocked kinetic-energ
 // consecutive records of each of its blocks in shared memory at a time (coalesced 256-byte loads), and each lane
 // then evaluates and adds its block's 32 (the evaluations are independent of the sums, so they overlap).
 constexpr int kPairSumWarps = 4;
+// The pair count is read from the device (the step's copy of the list's count, so a rebuild for the next step
+// cannot change it under the sums), capped at rec_cap, the records' buffer size, so the kernel can be recorded in a
+// CUDA graph with a grid for rec_cap; the block count goes to *nblocks_out for k_sum_pair_blocks.
 __global__ void __launch_bounds__(32 * kPairSumWarps) k_pair_block_sums(const double* __restrict__ pair_r2,
-                                                                        long long pairs, LJ lj,
-                                                                        double2* __restrict__ block_sums, int nblocks) {
+                                                                        const long long* __restrict__ pair_count,
+                                                                        long long rec_cap, LJ lj,
+                                                                        double2* __restrict__ block_sums,
+                                                                        int* __restrict__ nblocks_out) {
     __shared__ double tile[kPairSumWarps][32][33];
+    const long long pairs = *pair_count < rec_cap ? *pair_count : rec_cap;
+    const int nblocks = static_cast<int>((pairs + kChunk - 1) / kChunk);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *nblocks_out = nblocks;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b0 = (blockIdx.x * kPairSumWarps + warp) * 32;  // this warp's first block
     if (b0 >= nblocks) return;
@@ -181,10 +203,46 @@ __global__ void __launch_bounds__(32 * kPairSumWarps) k_pair_block_sums(const do
     if (b < nblocks) block_sums[b] = make_double2(se, sw);
 }
 
+// k_pair_block_sums over (pairEnergy, pairVirial) records (the force kernels' `terms` form): the same ordered
+// block sums, each lane adding its block's staged terms, with the same device pair count and block-count report.
+constexpr int kPairSumWarpsTerms = 2;
+__global__ void __launch_bounds__(32 * kPairSumWarpsTerms) k_pair_block_sums_terms(
+    const double2* __restrict__ pair_ew, const long long* __restrict__ pair_count, long long rec_cap,
+    double2* __restrict__ block_sums, int* __restrict__ nblocks_out) {
+    __shared__ double2 tile[kPairSumWarpsTerms][32][33];
+    const long long pairs = *pair_count < rec_cap ? *pair_count : rec_cap;
+    const int nblocks = static_cast<int>((pairs + kChunk - 1) / kChunk);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *nblocks_out = nblocks;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b0 = (blockIdx.x * kPairSumWarpsTerms + warp) * 32;  // this warp's first block
+    if (b0 >= nblocks) return;
+    double2(*t)[33] = tile[warp];
+    const int b = b0 + lane;
+    const long long k0 = static_cast<long long>(b) * kChunk;
+    const int m = b < nblocks ? static_cast<int>(pairs - k0 < kChunk ? pairs - k0 : kChunk) : 0;
+    double se = 0.0, sw = 0.0;
+    for (int c = 0; c < kChunk; c += 32) {
+        __syncwarp();
+        for (int r = 0; r < 32; ++r) {  // row r: records [c, c + 32) of block b0 + r, lane = record
+            const long long k = static_cast<long long>(b0 + r) * kChunk + c + lane;
+            t[r][lane] = b0 + r < nblocks && k < pairs ? pair_ew[k] : make_double2(0.0, 0.0);
+        }
+        __syncwarp();
+        const int e = m - c < 32 ? m - c : 32;
+        for (int u = 0; u < e; ++u) {
+            const double2 x = t[lane][u];
+            se = dadd(se, x.x);
+            sw = dadd(sw, x.y);
+        }
+    }
+    if (b < nblocks) block_sums[b] = make_double2(se, sw);
+}
+
 // The outer loop of deterministicSum (include/Parallel.hpp:52-56): block sums added in order from 0.0.
 // One warp: the lanes stage 256 values at a time in shared memory (the next chunk's loads in flight while
 // lane 0 adds the current one, one value after another, reading eight ahead of the adds).
-__global__ void k_sum_blocks(const double2* __restrict__ block_sums, int nblocks, double* __restrict__ out) {
+__device__ __forceinline__ void sum_blocks(const double2* __restrict__ block_sums, int nblocks,
+                                           double* __restrict__ out) {
     constexpr int kStage = 256;
     __shared__ double2 stage[kStage];
     const int lane = threadIdx.x & 31;
@@ -229,6 +287,22 @@ __global__ void k_sum_blocks(const double2* __restrict__ block_sums, int nblocks
         out[0] = se;
         out[1] = sw;
     }
+}
+
+__global__ void k_sum_blocks(const double2* __restrict__ block_sums, int nblocks, double* __restrict__ out) {
+    sum_blocks(block_sums, nblocks, out);
+}
+
+// sum_blocks over the 1024-pair blocks of k_pair_block_sums, as many as it reported
+__global__ void k_sum_pair_blocks(const double2* __restrict__ block_sums, const int* __restrict__ nblocks,
+                                  double* __restrict__ out) {
+    sum_blocks(block_sums, *nblocks, out);
+}
+
+// In a CUDA graph's list rebuild: the new list's pair count must fit the energy records' buffer, else the graph's
+// run repeats its steps on the host path (state[1], as k_build_done reports a row overflow)
+__global__ void k_pairs_fit(const long long* __restrict__ pair_count, long long rec_cap, int* __restrict__ state) {
+    if (*pair_count > rec_cap) state[1] = 1;
 }
 
 // ---- kinetic energy -----------------------------------------------------------------------------------

@@ -36,8 +36,9 @@ bool float_precision(int p) {
     return p == MD_PREC_FP32FX || p == MD_PREC_FP32 || p == MD_PREC_FX64 || p == MD_PREC_FX32;
 }
 
-// Step k (0-based) of a run of n_steps, as run_steps decides it
-RunStep plan_step(const md_run_options& o, int64_t k, int64_t n_steps, bool drifted_in) {
+// Step k (0-based) of a run of n_steps, as run_steps decides it (fusable: the float precisions, whose force kernel
+// can make the next step's kick and drift)
+RunStep plan_step(const md_run_options& o, int64_t k, int64_t n_steps, bool drifted_in, bool fusable) {
     RunStep r;
     const int64_t step = o.first_step + k;
     r.drifted_in = drifted_in;
@@ -45,15 +46,33 @@ RunStep plan_step(const md_run_options& o, int64_t k, int64_t n_steps, bool drif
     r.thermo = rescale ? 1 : (o.thermostat == 2 ? 2 : 0);
     r.target = rescale ? (step <= o.melt_until ? o.melt_temperature : o.rescale_temperature) : 0.0;
     r.rdf = o.rdf && o.rdf_every > 0 && step % o.rdf_every == 0;
-    r.fuse_out = k + 1 < n_steps && r.thermo == 0 && !r.rdf;
+    r.fuse_out = fusable && k + 1 < n_steps && r.thermo == 0 && !r.rdf;
     return r;
 }
 
-// Can md_run use graphs for this call? (float precisions on a tiled list built for this system; the tiled build
-// is the one the device rebuild enqueues)
+// The step's (PE, virial) into rec[0..1] on the stream where they end (FP64: the chain stream of its ordered sums),
+// as run_steps records them
+md_status record_energy(md_forcefield* ff, md_system* s, double* rec, bool want_energy) {
+    if (!want_energy) return MD_OK;
+    const cudaStream_t es = energy_stream(ff, s);
+    MD_CUDA(cudaMemcpyAsync(rec, ff->out.p, 2 * sizeof(double), cudaMemcpyDeviceToDevice, es));
+    if (es != s->stream) MD_CUDA(cudaEventRecord(ff->ev_done, es));  // the join covers the copy too
+    return MD_OK;
+}
+
+// MD_PREC_FP64 runs as graphs up to this many particles. Measured on the B200 (microseconds per step with energies
+// recorded, graph / host loop): 2,048: 79 / 99; 32,000: 87 / 105; 256,000: 293 / 318; 4,000,000: 3,253 / 2,410.
+// For a large list the ordered energy sums (a 1.1 ms chain at 4M) overlap the next steps on their own streams,
+// which a graph's branches did not match.
+constexpr int64_t kFp64GraphMaxParticles = 1'000'000;
+
+// Can md_run use graphs for this call? (a tiled list built for this system; the tiled build is the one the device
+// rebuild enqueues)
 bool graph_mode_ok(const md_system* s, const md_forcefield* ff, const md_nlist* nl, int64_t n_steps) {
-    return s->graph_chunk > 0 && n_steps > 0 && s->n > 0 && float_precision(ff->precision) && nlist_current(nl, s) &&
-           nl->use_cells && nl->use_tiles && nl->build_pin != 0;
+    const bool precision = float_precision(ff->precision) ||
+                           (ff->precision == MD_PREC_FP64 && s->n <= kFp64GraphMaxParticles);
+    return s->graph_chunk > 0 && n_steps > 0 && s->n > 0 && precision && nlist_current(nl, s) && nl->use_cells &&
+           nl->use_tiles && nl->build_pin != 0;
 }
 
 // Live data of a double-buffered array into its canonical buffer (recorded by the graphs); count elements
@@ -118,6 +137,16 @@ md_status graph_prepare_buffers(md_system* s, md_forcefield* ff, md_nlist* nl, c
         MD_CUDA(s->snap_hist.reserve(o.rdf->bins));
     }
     if (ff->precision == MD_PREC_FX32) MD_TRY(ensure_near_first(ff, s, nl));
+    if (ff->precision == MD_PREC_FP64) {
+        // the energy records of the lists a graph builds: a quarter more than the current list's pairs (a chunk
+        // whose rebuild outgrows them reruns on the host path, which grows them); the kinetic-energy blocks
+        MD_TRY(ensure_pairs(nl));
+        if (!ff->side) MD_TRY(energy_streams(ff));
+        MD_TRY(energy_quiesce(ff));
+        const long long pairs = static_cast<long long>(nl->pairs);
+        MD_TRY(reserve_energy_records(ff, pairs + pairs / 4 + kChunk));
+        MD_CUDA(s->ke_blocks.reserve(static_cast<size_t>((n + kChunk - 1) / kChunk)));
+    }
     // the resident grids of the force kernels that size their launch by occupancy, known before any capture
     int sms = 0;
     MD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
@@ -188,6 +217,15 @@ md_status device_rebuild_async(md_system* s, md_forcefield* ff, md_nlist* nl, co
     MD_CHECK_LAUNCH();
     k_build_done<<<1, 1, 0, st>>>(nl->flags.p + 1, nl->cap, s->graph_state.p, (s->graph_flags & MD_GRAPH_TEST_RERUN) != 0);
     MD_CHECK_LAUNCH();
+    if (ff->precision == MD_PREC_FP64) {  // the pair offsets of the energy records, and their count against the buffers
+        k_own_counts<<<blocks_for(n, kThreads), kThreads, 0, st>>>(nl->counts.p, n, nl->tmp_counts.p);
+        MD_CHECK_LAUNCH();
+        exclusive_scan<int, long long>(nl->tmp_counts.p, n, nl->half_off.p, nl->tiles.p, st);
+        MD_CHECK_SCAN();
+        const long long cap = static_cast<long long>(std::min(ff->pair_r2[0].count, ff->pair_r2[1].count) / 2);
+        k_pairs_fit<<<1, 1, 0, st>>>(nl->half_off.p + n, cap, s->graph_state.p);
+        MD_CHECK_LAUNCH();
+    }
     if (ff->precision == MD_PREC_FX32)  // the rows just built, split (the float frames are the build's)
         MD_TRY(split_rows_async(s, nl, nl->frames.p, static_cast<float>(nl->nf_near2), st));
     if (ff->precision == MD_PREC_FX64 || ff->precision == MD_PREC_FX32) {
@@ -233,7 +271,12 @@ std::string graph_key(const md_system* s, const md_forcefield* ff, const md_nlis
                           static_cast<const void*>(nl->grid.cursor.p), static_cast<const void*>(nl->grid.bucket.p),
                           static_cast<const void*>(nl->grid.order.p), static_cast<const void*>(nl->grid.tiles.p),
                           static_cast<const void*>(ff->fx_acc.p), static_cast<const void*>(ff->out.p),
-                          static_cast<const void*>(ff->inside_count.p),
+                          static_cast<const void*>(ff->inside_count.p), static_cast<const void*>(ff->pair_r2[0].p),
+                          static_cast<const void*>(ff->pair_r2[1].p), static_cast<const void*>(ff->eblocks[0].p),
+                          static_cast<const void*>(ff->eblocks[1].p), static_cast<const void*>(s->ke_blocks.p),
+                          static_cast<const void*>(ff->epairs.p), static_cast<const void*>(ff->enblocks.p),
+                          static_cast<const void*>(nl->half_off.p), static_cast<const void*>(nl->tmp_counts.p),
+                          static_cast<const void*>(nl->tiles.p),
                           static_cast<const void*>(o.rdf ? o.rdf->hist.p : nullptr)})
         ptr(p);
     for (double v : {static_cast<double>(s->n), s->box.L, static_cast<double>(nl->cap), static_cast<double>(tg.kk),
@@ -243,7 +286,8 @@ std::string graph_key(const md_system* s, const md_forcefield* ff, const md_nlis
                      want_ke ? 1.0 : 0.0, bussi_c, o.bussi_temperature, s->profile ? 1.0 : 0.0,
                      static_cast<double>(s->graph_chunk), o.rdf ? o.rdf->rmax : 0.0,
                      static_cast<double>(o.rdf ? o.rdf->bins : 0), static_cast<double>(ff->serial),
-                     static_cast<double>(nl->serial)})
+                     static_cast<double>(nl->serial), static_cast<double>(ff->pair_r2[0].count),
+                     static_cast<double>(ff->pair_r2[1].count)})
         num(v);
     for (const RunStep& r : steps) {
         std::snprintf(buf, sizeof buf, "%d%d%d%d", r.drifted_in, r.fuse_out, r.thermo, r.rdf);
@@ -299,7 +343,7 @@ md_status graph_step(md_system* s, md_forcefield* ff, md_nlist* nl, const md_run
     bool fused_ke = false;
     MD_TRY(forces_list_async(ff, s, nl, want_energy, dt, true, &fused_ke, r.fuse_out, r.drifted_in));
     double* rec = s->chunk_rec.p + 3 * static_cast<size_t>(k);
-    if (want_energy) MD_CUDA(cudaMemcpyAsync(rec, ff->out.p, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+    MD_TRY(record_energy(ff, s, rec, want_energy));
     bool ke_current = fused_ke;
     if (r.thermo) {
         if (!ke_current) MD_TRY(kinetic_async(s));
@@ -316,7 +360,7 @@ md_status graph_step(md_system* s, md_forcefield* ff, md_nlist* nl, const md_run
     }
     if (r.rdf) MD_TRY(rdf_kernel_async(o.rdf, s, nl));
     if (want_ke) {
-        if (!ke_current) MD_TRY(kinetic_fixed_async(s, ff));
+        if (!ke_current) MD_TRY(ff->precision == MD_PREC_FP64 ? kinetic_async(s) : kinetic_fixed_async(s, ff));
         MD_CUDA(cudaMemcpyAsync(rec + 2, s->scal.p + kScalKE, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
     }
     return MD_OK;
@@ -345,6 +389,10 @@ md_status chunk_graph(md_system* s, md_forcefield* ff, md_nlist* nl, const md_ru
     MD_CUDA(allow_smem(k_force_fp32_tile<true, false>, tile_smem));
     MD_CUDA(allow_smem(k_force_fp32_tile<false, true>, tile_smem));
     MD_CUDA(allow_smem(k_force_fp32_tile<false, false>, tile_smem));
+    MD_CUDA(allow_smem(k_force_fp64_tile<true>, sizeof(double4) * tg.max_staged));
+    MD_CUDA(allow_smem(k_force_fp64_tile<false>, sizeof(double4) * tg.max_staged));
+    // FP64: the capture starts with no energy sums queued and the records' first buffers (energy_quiesce)
+    MD_TRY(energy_quiesce(ff));
     if (s->profile) {
         rg.prof.resize(2 * steps.size());
         for (cudaEvent_t& ev : rg.prof) MD_CUDA(cudaEventCreate(&ev));
@@ -402,8 +450,20 @@ md_status chunk_graph(md_system* s, md_forcefield* ff, md_nlist* nl, const md_ru
             cp(nl->iframes2.p, nl->iframes.p, sizeof(int4) * N);
             swap_buffers(nl->iframes, nl->iframes2);
         }
+        // FP64: the energy sums' streams joined back into the graph's end
+        for (int b = 0; b < 2 && st == MD_OK; ++b) {
+            if (ff->read_pending[b] && cudaStreamWaitEvent(s->stream, ff->ev_read[b], 0) != cudaSuccess)
+                st = fail(MD_ERR_CUDA, "graph join of the block sums");
+            if (ff->chain_pending[b] && cudaStreamWaitEvent(s->stream, ff->ev_chain[b], 0) != cudaSuccess)
+                st = fail(MD_ERR_CUDA, "graph join of the ordered sums");
+        }
+        if (st == MD_OK && ff->side_pending && cudaStreamWaitEvent(s->stream, ff->ev_done, 0) != cudaSuccess)
+            st = fail(MD_ERR_CUDA, "graph join of the energy records");
         e = cudaStreamEndCapture(s->stream, &graph);
     }
+    // nothing the capture recorded has run: the host's record of queued sums starts afresh
+    const md_status eq = energy_quiesce(ff);
+    if (st == MD_OK) st = eq;
     g_capture_prof = saved_prof;
     g_graph_overflow = nullptr;
     g_capturing = false;
@@ -416,7 +476,8 @@ md_status chunk_graph(md_system* s, md_forcefield* ff, md_nlist* nl, const md_ru
         if (st != MD_OK) return st;
         return fail(MD_ERR_CUDA, std::string("md_run graph capture: ") + cudaGetErrorString(e));
     }
-    const cudaError_t ei = cudaGraphInstantiate(&rg.exec, graph, 0);
+    // per-node priorities: the FP64 energy sums' kernels carry the highest (launch_priority), as on their streams
+    const cudaError_t ei = cudaGraphInstantiate(&rg.exec, graph, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(graph);
     if (ei != cudaSuccess) {
         for (cudaEvent_t ev : rg.prof) cudaEventDestroy(ev);
@@ -437,11 +498,11 @@ std::vector<std::pair<int64_t, int64_t>> run_chunks(const md_system* s, int64_t 
     return c;
 }
 
-std::vector<RunStep> chunk_steps(const md_run_options& o, int64_t b, int64_t e, int64_t n_steps) {
+std::vector<RunStep> chunk_steps(const md_run_options& o, int64_t b, int64_t e, int64_t n_steps, bool fusable) {
     std::vector<RunStep> v;
     bool drifted = false;
     for (int64_t k = 0; k < e; ++k) {
-        const RunStep r = plan_step(o, k, n_steps, drifted);
+        const RunStep r = plan_step(o, k, n_steps, drifted, fusable);
         if (k >= b) v.push_back(r);
         drifted = r.fuse_out;
     }
@@ -456,8 +517,8 @@ md_status graph_prepare(md_system* s, md_forcefield* ff, md_nlist* nl, double dt
     const double bussi_c = o.thermostat == 2 ? std::exp(-dt / o.bussi_tau) : 0.0;
     for (const auto& c : run_chunks(s, nl->variant[ff->precision] < 0 ? 1 : 0, n_steps)) {
         RunGraph* g = nullptr;
-        MD_TRY(chunk_graph(s, ff, nl, o, chunk_steps(o, c.first, c.second, n_steps), dt, want_energy, want_ke, bussi_c,
-                           &g));
+        MD_TRY(chunk_graph(s, ff, nl, o, chunk_steps(o, c.first, c.second, n_steps, float_precision(ff->precision)), dt,
+                           want_energy, want_ke, bussi_c, &g));
     }
     return MD_OK;
 }
@@ -466,7 +527,7 @@ md_status graph_prepare(md_system* s, md_forcefield* ff, md_nlist* nl, double dt
 md_status host_step(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, int64_t n_steps, const md_run_options& o,
                     int64_t k, bool drifted_in, bool want_energy, bool want_ke, const double* noise, double* rec,
                     double bussi_c, bool* fused_out) {
-    const RunStep r = plan_step(o, k, n_steps, drifted_in);
+    const RunStep r = plan_step(o, k, n_steps, drifted_in, float_precision(ff->precision));
     bool rebuilt = false, fused_ke = false;
     if (drifted_in) {
         int flag = 0;
@@ -480,7 +541,7 @@ md_status host_step(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, in
     const bool fuse = r.fuse_out && nl->use_tiles && nlist_current(nl, s);
     MD_TRY(forces_list_async(ff, s, nl, want_energy, dt, true, &fused_ke, fuse, drifted_in && !rebuilt));
     *fused_out = fuse;
-    if (want_energy) MD_CUDA(cudaMemcpyAsync(rec + 3 * k, ff->out.p, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+    MD_TRY(record_energy(ff, s, rec + 3 * k, want_energy));
     bool ke_current = fused_ke;
     if (r.thermo) {
         if (!ke_current) MD_TRY(kinetic_async(s));
@@ -495,7 +556,7 @@ md_status host_step(md_system* s, md_forcefield* ff, md_nlist* nl, double dt, in
     }
     if (r.rdf) MD_TRY(rdf_sample_async(o.rdf, s, nl));
     if (want_ke) {
-        if (!ke_current) MD_TRY(kinetic_fixed_async(s, ff));
+        if (!ke_current) MD_TRY(ff->precision == MD_PREC_FP64 ? kinetic_async(s) : kinetic_fixed_async(s, ff));
         MD_CUDA(cudaMemcpyAsync(rec + 3 * k + 2, s->scal.p + kScalKE, sizeof(double), cudaMemcpyDeviceToDevice,
                                 s->stream));
     }
@@ -571,7 +632,7 @@ md_status run_steps_graph(md_system* s, md_forcefield* ff, md_nlist* nl, double 
     bool rebuilt_on_device = false;
     for (const auto& c : run_chunks(s, k0, n_steps)) {
         const int64_t b = c.first, e = c.second, len = e - b;
-        const std::vector<RunStep> steps = chunk_steps(o, b, e, n_steps);
+        const std::vector<RunStep> steps = chunk_steps(o, b, e, n_steps, float_precision(ff->precision));
         graphs = graphs && graph_mode_ok(s, ff, nl, n_steps) && steps.front().drifted_in == drifted;
         if (!graphs) {  // the host path for the rest of the run
             for (int64_t k = b; k < e; ++k)
@@ -587,6 +648,8 @@ md_status run_steps_graph(md_system* s, md_forcefield* ff, md_nlist* nl, double 
             MD_CUDA(cudaMemcpyAsync(s->chunk_noise.p + C, noise.p + n_steps + b, sizeof(double) * len,
                                     cudaMemcpyDeviceToDevice, s->stream));
         }
+        // the graph's FP64 energy sums use the records' first buffers: nothing queued may still read them
+        MD_TRY(energy_quiesce(ff));
         MD_CUDA(cudaGraphLaunch(g->exec, s->stream));
         MD_CUDA(cudaMemcpyAsync(s->host_scal, s->graph_state.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
         MD_TRY(sync(s));
@@ -622,6 +685,7 @@ md_status run_steps_graph(md_system* s, md_forcefield* ff, md_nlist* nl, double 
     }
     // the host's record of the tiles (their largest staged count) is stale after rebuilds on the device
     if (rebuilt_on_device) MD_TRY(tile_geometry(nl, s, &nl->use_tiles));
+    MD_TRY(join_energy(ff, s));  // records that host steps copied on an energy stream (FP64)
     if (pe || ke || virial) {
         std::vector<double> h(3 * static_cast<size_t>(n_steps));
         MD_CUDA(cudaMemcpyAsync(h.data(), rec.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s->stream));

@@ -407,11 +407,12 @@ __global__ void __launch_bounds__(kTileThreads) k_force_fp32_tile(
 // k_force_fp64 on a tile: the same per-particle order (own pairs in list order, then the pairs where the
 // particle is second, in increasing j) and the same double operation sequence, with neighbour positions
 // read from the staged tile. Optionally fuses the closing half kick (bit-identical to k_kick).
+template <bool kTerms>
 __global__ void __launch_bounds__(kTileThreads) k_force_fp64_tile(
     const double4* __restrict__ pos, int n_atoms, const int* __restrict__ cell_start,
     const int* __restrict__ cell_sorted, TileGeom g, LJ lj, const uint32_t* __restrict__ rows, int cap,
     const int2* __restrict__ counts, double* __restrict__ force, unsigned long long* __restrict__ inside,
-    KickArgs kick, const long long* __restrict__ half_off, double* __restrict__ pair_r2) {
+    KickArgs kick, const long long* __restrict__ half_off, double* __restrict__ pair_r2, long long rec_cap) {
     extern __shared__ double4 s_p[];
     __shared__ TileTables t;
     __shared__ int s_delta[kMaxSegment][32];
@@ -452,13 +453,13 @@ __global__ void __launch_bounds__(kTileThreads) k_force_fp64_tile(
             const double dz = min_image(dsub(a.z, b.z), g.box);
             const double r2 = norm2(dx, dy, dz);
             if (!(r2 < lj.rc2)) {
-                if (own && pair_r2) store_pair_r2(pair_r2, pb + s, r2);
+                if (own && pair_r2) store_pair_rec<kTerms>(pair_r2, pb + s, r2, 0.0, 0.0, false, rec_cap);
                 continue;
             }
             double f, en;
             pair_terms(r2, lj, f, en);
             if (own) {
-                if (pair_r2) store_pair_r2(pair_r2, pb + s, r2);
+                if (pair_r2) store_pair_rec<kTerms>(pair_r2, pb + s, r2, f, en, true, rec_cap);
                 fx = dadd(fx, dmul(f, dx));
                 fy = dadd(fy, dmul(f, dy));
                 fz = dadd(fz, dmul(f, dz));

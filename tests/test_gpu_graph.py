@@ -1,4 +1,4 @@
-"""md_run as CUDA graphs (float precisions on a tiled list): every step of a chunk, the list rebuild decided on the
+"""md_run as CUDA graphs (every precision on a tiled list): every step of a chunk, the list rebuild decided on the
 device in a conditional node, the thermostat and the g(r) sample included. The graph path must give the host
 loop's trajectory bit for bit (the host loop is md_system_set_graph(s, 0), and md_step_list one step at a time),
 also when a device rebuild outgrows the recorded tile and the chunk reruns on the host path."""
@@ -11,7 +11,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-PRECS = ["PREC_FP32FX", "PREC_FP32", "PREC_FX64", "PREC_FX32"]
+PRECS = ["PREC_FP32FX", "PREC_FP32", "PREC_FX64", "PREC_FX32", "PREC_FP64"]
 
 
 def start(md, cells=12, temperature=1.3, seed=5):
@@ -48,7 +48,7 @@ def test_graph_run_matches_step_list(md, prec):
     assert s.state_hash() == r.state_hash()
 
 
-@pytest.mark.parametrize("prec", ["PREC_FP32FX", "PREC_FX32"])
+@pytest.mark.parametrize("prec", ["PREC_FP32FX", "PREC_FX32", "PREC_FP64"])
 @pytest.mark.parametrize("thermostat", ["rescale", "bussi"])
 def test_graph_run_with_thermostat_and_rdf_matches_host_loop(md, prec, thermostat):
     """Rescale (melt schedule, every 7 steps) or Bussi NVT, with a g(r) sample every 5 steps: per-step PE, KE and
@@ -76,7 +76,7 @@ def test_graph_run_with_thermostat_and_rdf_matches_host_loop(md, prec, thermosta
         assert np.array_equal(sa[k], sb[k]), k
 
 
-@pytest.mark.parametrize("prec", ["PREC_FP32FX", "PREC_FX32"])
+@pytest.mark.parametrize("prec", ["PREC_FP32FX", "PREC_FX32", "PREC_FP64"])
 def test_graph_overflow_reruns_chunk_on_host_path(md, prec):
     """With the test flag, every device rebuild reports an overflow (as a row past the capacity or a cell past the
     recorded tile would); each chunk that rebuilds starts again from its snapshot on the host path. The trajectory
