@@ -162,16 +162,18 @@ constexpr int kEnergyWarps = 4;  // warps per block of the blocked kinetic-energ
 // consecutive records of each of its blocks in shared memory at a time (coalesced 256-byte loads), and each lane
 // then evaluates and adds its block's 32 (the evaluations are independent of the sums, so they overlap).
 constexpr int kPairSumWarps = 4;
-// The pair count is read from the device (the step's copy of the list's count, so a rebuild for the next step
-// cannot change it under the sums), capped at rec_cap, the records' buffer size, so the kernel can be recorded in a
-// CUDA graph with a grid for rec_cap; the block count goes to *nblocks_out for k_sum_pair_blocks.
+// The pair count is rec_cap, or, in a CUDA graph (where it is known only on the device), read from *pair_count
+// (the step's copy of the list's count, so a rebuild for the next step cannot change it under the sums) and capped
+// at rec_cap, the records' buffer size; the grid then covers rec_cap. The block count goes to *nblocks_out for
+// k_sum_pair_blocks.
 __global__ void __launch_bounds__(32 * kPairSumWarps) k_pair_block_sums(const double* __restrict__ pair_r2,
                                                                         const long long* __restrict__ pair_count,
                                                                         long long rec_cap, LJ lj,
                                                                         double2* __restrict__ block_sums,
                                                                         int* __restrict__ nblocks_out) {
     __shared__ double tile[kPairSumWarps][32][33];
-    const long long pairs = *pair_count < rec_cap ? *pair_count : rec_cap;
+    const long long count = pair_count ? *pair_count : rec_cap;
+    const long long pairs = count < rec_cap ? count : rec_cap;
     const int nblocks = static_cast<int>((pairs + kChunk - 1) / kChunk);
     if (blockIdx.x == 0 && threadIdx.x == 0) *nblocks_out = nblocks;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -210,7 +212,8 @@ __global__ void __launch_bounds__(32 * kPairSumWarpsTerms) k_pair_block_sums_ter
     const double2* __restrict__ pair_ew, const long long* __restrict__ pair_count, long long rec_cap,
     double2* __restrict__ block_sums, int* __restrict__ nblocks_out) {
     __shared__ double2 tile[kPairSumWarpsTerms][32][33];
-    const long long pairs = *pair_count < rec_cap ? *pair_count : rec_cap;
+    const long long count = pair_count ? *pair_count : rec_cap;
+    const long long pairs = count < rec_cap ? count : rec_cap;
     const int nblocks = static_cast<int>((pairs + kChunk - 1) / kChunk);
     if (blockIdx.x == 0 && threadIdx.x == 0) *nblocks_out = nblocks;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -298,6 +301,9 @@ __global__ void k_sum_pair_blocks(const double2* __restrict__ block_sums, const 
                                   double* __restrict__ out) {
     sum_blocks(block_sums, *nblocks, out);
 }
+
+// The step's pair count into the slot its energy sums read
+__global__ void k_copy_count(const long long* __restrict__ from, long long* __restrict__ to) { *to = *from; }
 
 // In a CUDA graph's list rebuild: the new list's pair count must fit the energy records' buffer, else the graph's
 // run repeats its steps on the host path (state[1], as k_build_done reports a row overflow)
