@@ -178,6 +178,11 @@ md_status md_nlist_layout(const md_nlist* nl, int* use_tiles, int* segment_cells
  * rev_pairs[pairs] (pairsAsSecond). Any may be NULL. */
 md_status md_nlist_download(md_nlist* nl, uint64_t* offsets, uint64_t* neighbours, uint64_t* rev_offsets,
                             uint64_t* rev_pairs);
+/* MD_PREC_FX32's split of the last build's rows (diagnostics; the reference has no counterpart): near_rows[n * 16]
+ * and far_rows[n * row_capacity], row i's entries in order (j | cell code << 27, the sentinel j = n), groups[2 n]
+ * = (near groups, far groups) of 8 entries, near2 = the squared radius that classified them. MD_ERR_STATE until
+ * MD_PREC_FX32 forces have been computed on this build. Any pointer may be NULL. */
+md_status md_nlist_fx32_rows(md_nlist* nl, uint32_t* near_rows, uint32_t* far_rows, int32_t* groups, double* near2);
 
 /* ---- LennardJonesForceField: include/Forcefield.hpp:8-45, src/Forcefield.cpp ------------------------ */
 /* LennardJonesForceField(epsilon, sigma, cut_off) (src/Forcefield.cpp:8-15). Precision starts at MD_PREC_FP64. */

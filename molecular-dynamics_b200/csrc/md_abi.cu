@@ -1449,6 +1449,36 @@ md_status md_nlist_download(md_nlist* nl, uint64_t* offsets, uint64_t* neighbour
     return MD_OK;
 }
 
+md_status md_nlist_fx32_rows(md_nlist* nl, uint32_t* near_rows, uint32_t* far_rows, int32_t* groups, double* near2) {
+    if (!nl) return fail(MD_ERR_INVALID, "null list");
+    if (!nl->built || nl->nf_build != nl->builds || !(nl->nf_near2 > 0.0))
+        return fail(MD_ERR_STATE, "md_nlist_fx32_rows: the last build has no MD_PREC_FX32 split (compute its forces first)");
+    MD_TRY(use_system(const_cast<md_system*>(nl->sys)));
+    const long long n = static_cast<long long>(nl->n);
+    const int cap = nl->cap;
+    cudaStream_t st = nl->sys->stream;
+    if (near2) *near2 = nl->nf_near2;
+    // rows_nf: the near rows (capacity kFx32NearCap), then the far rows (capacity cap), both interleaved (entry s
+    // of row i at ((i >> 5) * (c >> 2) + (s >> 2)) * 128 + (i & 31) * 4 + (s & 3) for capacity c)
+    auto copy_rows = [&](size_t first, int c, uint32_t* out) -> md_status {
+        std::vector<uint32_t> raw(row_buffer_entries(n, c));
+        if (raw.empty()) return MD_OK;
+        MD_CUDA(cudaMemcpyAsync(raw.data(), nl->rows_nf.p + first, sizeof(uint32_t) * raw.size(), cudaMemcpyDeviceToHost, st));
+        MD_CUDA(cudaStreamSynchronize(st));
+        for (long long i = 0; i < n; ++i)
+            for (int s = 0; s < c; ++s)
+                out[i * c + s] = raw[((static_cast<size_t>(i >> 5) * (c >> 2) + (s >> 2)) * 32 + (i & 31)) * 4 + (s & 3)];
+        return MD_OK;
+    };
+    if (near_rows) MD_TRY(copy_rows(0, kFx32NearCap, near_rows));
+    if (far_rows) MD_TRY(copy_rows(fx32_near_entries(n), cap, far_rows));
+    if (groups && n > 0) {
+        MD_CUDA(cudaMemcpyAsync(groups, nl->counts_nf.p, sizeof(int2) * n, cudaMemcpyDeviceToHost, st));
+        MD_CUDA(cudaStreamSynchronize(st));
+    }
+    return MD_OK;
+}
+
 // ---- LennardJonesForceField --------------------------------------------------------------------------------
 
 md_status md_forcefield_create(double epsilon, double sigma, double cutoff, md_forcefield** out) {

@@ -70,6 +70,7 @@ def _load():
         "md_nlist_set_force_variant": (_I, [_P, _I, _I]), "md_nlist_force_variant": (_I, [_P, _I, _PI]),
         "md_nlist_set_build_variant": (_I, [_P, _I]), "md_nlist_build_variant": (_I, [_P, _PI]),
         "md_nlist_download": (_I, [_P, _PU64, _PU64, _PU64, _PU64]),
+        "md_nlist_fx32_rows": (_I, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _PI, _PD]),
         "md_forcefield_create": (_I, [_D, _D, _D, _PP]), "md_forcefield_destroy": (_I, [_P]),
         "md_forcefield_shift": (_I, [_P, _PD]), "md_forcefield_set_precision": (_I, [_P, _I]),
         "md_forcefield_set_deterministic": (_I, [_P, _I]),
@@ -417,6 +418,20 @@ class NeighbourList:
         rp = np.zeros(P, dtype=np.uint64) if rev else None
         _check(LIB.md_nlist_download(self.h, _pu(off), _pu(nb), _pu(roff), _pu(rp)))
         return dict(offsets=off, neighbours=nb, rev_offsets=roff, rev_pairs=rp)
+
+    def fx32_rows(self):
+        """MD_PREC_FX32's near and far rows of the last build (diagnostics): entries j | code << 27 per row in
+        order (near: 16 slots, far: row_capacity slots), (near groups, far groups) per particle and the squared
+        radius that classified them. Raises until MD_PREC_FX32 forces were computed on this build."""
+        n, cap = self.n, self.layout()["row_capacity"]
+        near = np.zeros((n, 16), dtype=np.uint32)
+        far = np.zeros((n, cap), dtype=np.uint32)
+        groups = np.zeros((n, 2), dtype=np.int32)
+        near2 = C.c_double()
+        u32 = C.POINTER(C.c_uint32)
+        _check(LIB.md_nlist_fx32_rows(self.h, near.ctypes.data_as(u32), far.ctypes.data_as(u32), _pi(groups),
+                                      C.byref(near2)))
+        return dict(near=near, far=far, groups=groups, near2=near2.value)
 
 
 class LennardJonesForceField:
