@@ -150,3 +150,29 @@ def test_fx32_split_rows_after_graph_rebuilds(md):
                           np.where(slots[:, :NEAR_CAP] < 8 * host["groups"][:, :1], host["near"], 0))
     assert np.array_equal(np.where(slots < 8 * split["groups"][:, 1:], split["far"], 0),
                           np.where(slots < 8 * host["groups"][:, 1:], host["far"], 0))
+
+
+def test_fx32_split_rows_ragged(md):
+    """A ragged start: 1,001 particles (the last 32-row group of the interleaved layouts part full) at uneven
+    density, one of them alone in a hole (an empty row: no near and no far groups)."""
+    base = md.fcc_system(8, 0.8442, 1.0, seed=3)
+    box, pos = base.box, base.download()["pos"][:, :3]
+    centre = np.full(3, box / 2)
+    d = pos - centre
+    d -= box * np.round(d / box)
+    rng = np.random.default_rng(9)
+    keep = rng.choice(np.flatnonzero((d * d).sum(axis=1) > 4.0 ** 2), 1000, replace=False)
+    p = np.zeros((1001, 4))
+    p[:1000, :3] = pos[keep]
+    p[1000, :3] = centre
+    s = md.System.from_arrays(p, box)
+    nl = md.NeighbourList(2.5, 0.3)
+    nl.build(s)
+    md.LennardJonesForceField(1.0, 1.0, 2.5, precision=md.PREC_FX32).compute_forces(s, nl)
+    split = nl.fx32_rows()
+    n = s.n
+    rows = full_rows(nl, n)
+    exact, _ = check_rows(rows, split, n, nl.layout()["row_capacity"], s.download()["pos"], s.box)
+    assert exact >= 0.95 * n
+    empty = [i for i, r in enumerate(rows) if not r]
+    assert empty and all(tuple(split["groups"][i]) == (0, 0) for i in empty)
